@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the jaxframes distributed-algorithms hot path on B200.
+
+Headline workload: sort-merge inner join, left 10M rows (int64 key uniform in
+[0, 5M), float32 payload), right 5M rows (key = a permutation of 0..5M-1,
+int32 payload over the full int32 range), output (left_idx, right_idx) pairs
+plus the gathered payloads -- one step is one ``ParallelSortMergeJoin.join``
+through the public API.  Inputs are synthetic (``np.random.default_rng(43)``)
+and larger than L2 (180 MB resident), so no L2 flush is needed between steps.
+
+``value`` = input rows (left + right) per second over the whole job with
+inputs resident in HBM; ``e2e`` = the same through the API from pinned host
+buffers, host<->device copies included.  ``--impl reference`` times the
+reference's algorithm on the host CPU (the NumPy restatement; jaxframes itself
+needs jax, which is not installed) on a bounded sample.
+
+Prints one JSON line (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NL, NR = 10_000_000, 5_000_000
+METRIC = "sort-merge inner join throughput (input rows/s)"
+WORKLOAD = "sort-merge inner join 10M x 5M int64 keys, f32 + i32 payloads"
+
+
+def make_join_inputs(nl=NL, nr=NR, seed=43):
+    rng = np.random.default_rng(seed)
+    lk = rng.integers(0, nr, nl, dtype=np.int64)
+    lv = rng.standard_normal(nl, dtype=np.float32)
+    rk = rng.permutation(nr).astype(np.int64)
+    rv = rng.integers(-2**31, 2**31, nr, dtype=np.int64).astype(np.int32)
+    return lk, lv, rk, rv
+
+
+def c3_inputs(n=100_000_000, seed=44):
+    """Multi-key groupby input: k1 truncated Zipf(s=1.1) over 1M ranks mapped
+    through a permutation, k2 uniform in [0, 64), v1 N(0,1) float32, v2 uniform
+    int64 in [-1e6, 1e6]."""
+    rng = np.random.default_rng(seed)
+    ranks = np.arange(1, 1_000_001, dtype=np.float64)
+    cdf = np.cumsum(ranks ** -1.1)
+    cdf /= cdf[-1]
+    perm = rng.permutation(1_000_000).astype(np.int32)
+    k1 = perm[np.searchsorted(cdf, rng.random(n))]
+    k2 = rng.integers(0, 64, n, dtype=np.int64).astype(np.int32)
+    v1 = rng.standard_normal(n, dtype=np.float32)
+    v2 = rng.integers(-1_000_000, 1_000_001, n, dtype=np.int64)
+    return k1, k2, v1, v2
+
+
+def join_model_bytes(nl, nr, m):
+    """Algorithmic bytes of the join: SORT(L) + SORT(R) + merge read + output,
+    with K = 8 (int64 key), I = 4, P = ceil(23 / 11) = 3 passes."""
+    K, I, P = 8, 4, 3
+    sort = lambda n: n * (8 + (K + I) + (P - 1) * 2 * (K + I))
+    return sort(nl) + sort(nr) + (nl + nr) * (K + I) + m * (2 * I + K + 4 + 4 + 4 + 4)
+
+
+# ------------------------------------------------------------------ clocks ---
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU legs ---
+def cpu_join_sample(nl, nr, seconds=10.0):
+    """Single-threaded oracle join on a sample; rows/s."""
+    from oracle import jfx_oracle as O
+    lk, lv, rk, rv = make_join_inputs(nl, nr, seed=44)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.sort_merge_join(lk, {"lv": lv}, rk, {"rv": rv}, "inner")
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= 50:
+            break
+    return (nl + nr) * reps / el, reps
+
+
+_REF = {}
+
+
+def _ref_worker(p):
+    from oracle import jfx_oracle as O
+    lk, lv, rk, rv, lp, rp = (_REF[k] for k in ("lk", "lv", "rk", "rv", "lp", "rp"))
+    li = np.flatnonzero(lp == p)
+    ri = np.flatnonzero(rp == p)
+    mk, out, _, _ = O.sort_merge_join(lk[li], {"lv": lv[li]}, rk[ri], {"rv": rv[ri]}, "inner")
+    return len(mk)
+
+
+def run_reference(args):
+    """The reference's algorithm on the host CPU: the oracle restatement of
+    ParallelSortMergeJoin.join on a sample of the workload, hash-partitioned
+    across all available cores (one process per core)."""
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0))
+    nl, nr = NL // 5, NR // 5
+    lk, lv, rk, rv = make_join_inputs(nl, nr, seed=44)
+    _REF.update(lk=lk, lv=lv, rk=rk, rv=rv, lp=(lk % cores).astype(np.int32), rp=(rk % cores).astype(np.int32))
+    ctx = mp.get_context("fork")  # this arm never initialises CUDA
+    times = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            m = sum(pool.map(_ref_worker, range(cores)))
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+    ms = 1000 * statistics.mean(times)
+    value = (nl + nr) / (ms / 1000)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{nl} x {nr} rows per step", "parallelism": f"{cores} processes"},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cores, "kind": "port",
+                         "sample": f"inner join {nl} x {nr} rows, hash-partitioned over {cores} processes; "
+                                   "NumPy restatement of parallel_algorithms.py:938-1075 (jax not installed)"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "matched_rows": m,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- GPU ---
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from jaxframes_b200 import build as b
+    if rank == 0 or world == 1:
+        b.build()
+    if world > 1:
+        dist.barrier()
+    from jaxframes_b200 import _lib
+    import jaxframes_b200.parallel_algorithms as P
+    L = _lib.load_library()
+
+    lk, lv, rk, rv = make_join_inputs()
+    dev = torch.device("cuda", local)
+    d_lk, d_lv = torch.from_numpy(lk).to(dev), torch.from_numpy(lv).to(dev)
+    d_rk, d_rv = torch.from_numpy(rk).to(dev), torch.from_numpy(rv).to(dev)
+    joiner = P.ParallelSortMergeJoin()
+
+    def step():
+        return joiner.join(d_lk, {"lv": d_lv}, d_rk, {"rv": d_rv}, "inner")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        mk, out = step()
+    torch.cuda.synchronize()
+    m_rows = int(mk.numel())
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = L.jfx_launch_count()
+    L.jfx_timing_enable(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        mk, out = step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    launches = int(L.jfx_launch_count() - launches0)
+    import ctypes
+    pms, pl, pb = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+    L.jfx_timing_read(ctypes.byref(pms), ctypes.byref(pl), ctypes.byref(pb))
+    L.jfx_timing_enable(0)
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # end to end: pinned host buffers in, results back to the host
+    h = [torch.from_numpy(x).pin_memory() for x in (lk, lv, rk, rv)]
+    h2d = sum(x.numel() * x.element_size() for x in h)
+
+    def e2e_step():
+        mk, out = joiner.join(h[0], {"lv": h[1]}, h[2], {"rv": h[3]}, "inner")
+        r = [mk.cpu(), out["left_lv"].cpu(), out["right_rv"].cpu()]
+        return sum(x.numel() * x.element_size() for x in r)
+
+    for _ in range(max(1, args.warmup // 2)):
+        d2h = e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 5))
+    f0.record()
+    for _ in range(e2e_steps):
+        d2h = e2e_step()
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    pass_ms = pms.value / max(pl.value, 1)
+    pass_bytes = pb.value / max(pl.value, 1)
+    achieved = pass_bytes / (pass_ms / 1000) / 1e9 if pass_ms > 0 else None
+    rows = (NL + NR) * world
+    value = rows / (ms / 1000)
+    model = join_model_bytes(NL, NR, m_rows)
+
+    extra = {}
+    if args.extra and rank == 0 and world == 1:
+        extra = run_extra(args, P, dev)
+
+    if rank == 0:
+        cpu_v, reps = cpu_join_sample(NL // 10, NR // 10, seconds=args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "left_rows": NL, "right_rows": NR, "output_rows": m_rows,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs 180 MB > 126 MB L2, no flush"},
+            "model_gbs": model / (ms / 1000) / 1e9,
+            "model_frac": model / (ms / 1000) / 1e9 / hbm,
+            "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix pass)", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                         "traffic": None, "peak_source": peak_src,
+                         "launches": int(pl.value), "avg_launch_ms": pass_ms},
+            "e2e": {"value": (NL + NR) * world / (e2e_ms / 1000), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": {"value": cpu_v, "unit": "rows/s", "cores": 1, "kind": "port",
+                             "sample": f"inner join {NL // 10} x {NR // 10} rows x {reps} reps, single-threaded "
+                                       "NumPy restatement (jax not installed)"},
+        }
+        if extra:
+            line["extra"] = extra
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_extra(args, P, dev):
+    """Secondary measurements on the other configs (not the headline)."""
+    import torch
+    out = {}
+
+    def timeit(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b2.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b2) / steps
+
+    try:
+        rng = np.random.default_rng(42)
+        n = 1_000_000
+        k = torch.from_numpy(rng.integers(0, 1000, n).astype(np.int32)).to(dev)
+        v = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+        ms = timeit(lambda: P.groupby_aggregate(k, {"v": v, "c": v}, {"v": "sum", "c": "count"}), 5)
+        out["groupby_sum_1M"] = {"ms": ms, "rows_per_s": n / (ms / 1e3)}
+    except Exception as e:  # report, do not hide
+        out["groupby_sum_1M"] = {"error": repr(e)}
+    try:
+        k1, k2, v1, v2 = [torch.from_numpy(x).to(dev) for x in c3_inputs()]
+        vals = {f"v1_{a}": v1 for a in ("sum", "mean", "min", "max", "count")}
+        vals.update({f"v2_{a}": v2 for a in ("sum", "mean", "min", "max", "count")})
+        aggs = {c: c.split("_")[1] for c in vals}
+        res = {}
+        ms = timeit(lambda: res.setdefault("r", P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)),
+                    3)
+        g = int(P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)[0]["k1"].numel())
+        n = k1.numel()
+        model = n * (8 + 8 + 2 * 2 * 8) + n * (4 + 4 + 4 + 8) + g * 60
+        out["groupby_multikey_100M"] = {"ms": ms, "rows_per_s": n / (ms / 1e3), "groups": g,
+                                        "model_gbs": model / (ms / 1e3) / 1e9}
+        del k1, k2, v1, v2, vals
+    except Exception as e:
+        out["groupby_multikey_100M"] = {"error": repr(e)}
+    try:
+        rng = np.random.default_rng(45)
+        n = 1 << 28
+        keys = torch.from_numpy(rng.integers(0, 2**63, n, dtype=np.uint64)).to(dev)
+        s = P.ParallelRadixSort()
+        ms = timeit(lambda: s.argsort(keys), 2)
+        model = n * (8 + 12 + 5 * 24)
+        out["sort_u64_256M_uniform"] = {"ms": ms, "keys_per_s": n / (ms / 1e3), "model_gbs": model / (ms / 1e3) / 1e9}
+        del keys
+    except Exception as e:
+        out["sort_u64_256M_uniform"] = {"error": repr(e)}
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="jfx", choices=["jfx", "reference"])
+    ap.add_argument("--extra", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * jfx.h -- C ABI of the B200 (sm_100a) kernels behind jaxframes' distributed
+ * algorithms layer (src/jaxframes/distributed/parallel_algorithms.py).
+ *
+ * Every entry point takes plain device pointers, element counts, a caller-owned
+ * device workspace (size from jfx_workspace_size) and a cudaStream_t passed as
+ * void*.  Work is stream-ordered; entry points that must size an output (group
+ * count, join pair count) synchronise the stream once and return the size
+ * through a host pointer, as the reference does with its host reads at
+ * parallel_algorithms.py:712, :772 and :880.
+ *
+ * Return value: JFX_OK (0) or a negative jfx_status; jfx_last_error() gives a
+ * thread-local message.  Nothing here falls back to the CPU.
+ */
+#ifndef JFX_H
+#define JFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  JFX_OK = 0,
+  JFX_ERR_ARG = -1,      /* bad argument (null pointer, bad count, bad flag) */
+  JFX_ERR_DTYPE = -2,    /* dtype the reference does not sort / aggregate */
+  JFX_ERR_ALLOC = -3,    /* workspace too small */
+  JFX_ERR_TIMEOUT = -4,  /* a bounded device-side wait gave up */
+  JFX_ERR_CAPACITY = -5, /* output capacity or row limit exceeded */
+  JFX_ERR_CUDA = -6      /* CUDA runtime error */
+} jfx_status;
+
+typedef enum {
+  JFX_I8 = 1, JFX_I16 = 2, JFX_I32 = 3, JFX_I64 = 4,
+  JFX_U8 = 5, JFX_U16 = 6, JFX_U32 = 7, JFX_U64 = 8,
+  JFX_F32 = 9, JFX_F64 = 10, JFX_BOOL = 11
+} jfx_dtype;
+
+/* column flags */
+#define JFX_COL_DESC 1u /* descending key of multi_column_lexsort (-x / max-x) */
+
+typedef struct {
+  const void* data; /* device pointer, n elements, contiguous */
+  int32_t dtype;    /* jfx_dtype */
+  uint32_t flags;   /* JFX_COL_* */
+} jfx_column;
+
+/* aggregation bits (SortBasedGroupBy._apply_aggregation_vectorized,
+ * parallel_algorithms.py:626-660, and _scatter_group_aggregate, :1212-1228) */
+#define JFX_AGG_SUM 1u
+#define JFX_AGG_MEAN 2u
+#define JFX_AGG_COUNT 4u
+#define JFX_AGG_MIN 8u
+#define JFX_AGG_MAX 16u
+
+typedef struct {
+  const void* data; /* device pointer to the value column (original row order) */
+  int32_t dtype;    /* jfx_dtype of the values */
+  uint32_t aggs;    /* JFX_AGG_* bits requested on this column */
+  /* outputs, capacity n each, indexed by group; dtypes follow the reference:
+   * sum: value dtype; count: value dtype (single key) or int32 (multi key);
+   * mean: mean_dtype; min/max: value dtype */
+  void* out_sum;
+  void* out_mean;
+  void* out_count;
+  void* out_min;
+  void* out_max;
+  int32_t mean_dtype; /* JFX_F32 or JFX_F64 */
+  int32_t count_dtype;
+} jfx_agg_column;
+
+/* join kinds (ParallelSortMergeJoin.join, parallel_algorithms.py:938-1075) */
+#define JFX_JOIN_INNER 0
+#define JFX_JOIN_LEFT 1
+#define JFX_JOIN_RIGHT 2
+#define JFX_JOIN_OUTER 3
+
+/* workspace kinds for jfx_workspace_size */
+#define JFX_WS_SORT 1      /* n1 = rows */
+#define JFX_WS_GROUPBY 2   /* n1 = rows */
+#define JFX_WS_JOIN 3      /* n1 = left rows, n2 = right rows */
+#define JFX_WS_PARTITION 4 /* n1 = rows, n2 = partitions */
+#define JFX_WS_LEARNED 5   /* n1 = rows (uint64 keys) */
+
+const char* jfx_last_error(void);
+int jfx_version(void);
+int jfx_max_rows(void);
+size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2);
+
+/* ParallelRadixSort.sort (parallel_algorithms.py:463-581) / parallel_sort
+ * (:1079-1114): stable ascending order of `key`; ascending==0 reverses the
+ * whole result.  Writes the permutation (int32 row ids) and, if non-null, the
+ * sorted keys in the key's dtype. */
+int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
+             void* sorted_keys_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* multi_column_lexsort (parallel_algorithms.py:25-66): stable lexicographic
+ * argsort of ncols columns (first column most significant), JFX_COL_DESC per
+ * column.  One column: ascending ignored, as in the reference. */
+int jfx_lexsort(const jfx_column* keys, int ncols, int64_t n, int32_t* perm_out,
+                void* workspace, size_t workspace_bytes, void* stream);
+
+/* SortBasedGroupBy.groupby_aggregate (:733-803, multi_key=0) and
+ * groupby_aggregate_multi_column (:662-731, multi_key=1).  unique_out[c] gets
+ * the unique keys of column c (capacity n, ascending / lexicographic order).
+ * *num_groups receives G after one stream synchronisation. */
+int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key,
+                const jfx_agg_column* values, int nvalues, void* const* unique_out,
+                int64_t* num_groups, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Opaque state passed from jfx_join_prepare to jfx_join_expand (caller-owned,
+ * plain memory; it points into the workspace, which must stay untouched). */
+typedef struct {
+  uint64_t opaque[64];
+} jfx_join_plan;
+
+/* ParallelSortMergeJoin.join (:938-1075), first half: radix sorts both key
+ * columns with one shared key packing and counts the output rows for `how`
+ * (JFX_JOIN_INNER / LEFT / RIGHT).  *num_out receives the row count after one
+ * stream synchronisation. */
+int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* right_key,
+                     int64_t nr, int how, jfx_join_plan* plan, int64_t* num_out,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Second half: writes num_out rows of (left row id, right row id) -- -1 for a
+ * missing side -- and, if keys_out is non-null, the merged key column (key
+ * dtype).  Row order is the reference's: inner pairs by (key, left row, right
+ * row); left/right rows in that side's sorted order with the first match of
+ * the other side. */
+int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out,
+                    void* keys_out, void* stream);
+
+/* Payload gather with the reference's join fill (:1056-1073): out[i] =
+ * src[idx[i]] converted to out_dtype, NaN where idx[i] < 0 (float outputs). */
+int jfx_gather(const void* src, int32_t src_dtype, int64_t n_src, const int32_t* idx,
+               int64_t n, void* out, int32_t out_dtype, void* stream);
+
+/* hash_multi_columns (parallel_algorithms.py:69-136): uint32 per row. */
+int jfx_hash_columns(const jfx_column* keys, int ncols, int64_t n, uint32_t* hash_out,
+                     void* stream);
+
+/* One device's body of collective_hash_repartition (:163-182, :213-214) with
+ * the device count set to num_partitions: target = hash % P and a stable
+ * counting sort by target.  Writes targets (nullable), the permutation and
+ * offsets[P+1] (int64). */
+int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_partitions,
+                       int32_t* targets_out, int32_t* perm_out, int64_t* offsets_out,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Measurement hooks.  No counterpart in the reference, which has no tracing.
+ * jfx_launch_count: number of kernels this library has launched so far.
+ * jfx_timing_enable(1) clears and starts CUDA-event timing of the radix pass
+ * kernels on their launching streams; jfx_timing_read waits for the recorded
+ * launches and returns their summed duration, count and algorithmic bytes. */
+uint64_t jfx_launch_count(void);
+int jfx_timing_enable(int enable);
+int jfx_timing_read(double* total_ms, int64_t* launches, double* algo_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JFX_H */

@@ -1,0 +1,659 @@
+// api.cu -- extern "C" entry points of libjfx (declared in include/jfx.h).
+#include "join.cuh"
+
+namespace jfx {
+
+thread_local std::string g_last_error;
+thread_local HostScratch g_host;
+std::atomic<unsigned long long> g_launches{0};
+Timing g_timing;
+
+int device_sm_count() {
+  static int cache[128] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 128) return 148;
+  if (!cache[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cache[dev] = v;
+  }
+  return cache[dev];
+}
+
+static inline cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+static inline int grid_for(u64 n, int threads) {
+  u64 g = (n + threads - 1) / threads;
+  u64 cap = (u64)device_sm_count() * 16;
+  return (int)std::max<u64>(1, std::min(g, cap));
+}
+
+// Copies the device error word (and up to 3 more words) back, synchronising
+// the stream once, and converts device error bits into a status.
+static int read_back(const void* dev, size_t bytes, u64* host, cudaStream_t s) {
+  JFX_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  return JFX_OK;
+}
+
+static int check_err_word(u32 e) {
+  if (e & DERR_TIMEOUT)
+    return fail(JFX_ERR_TIMEOUT, "a device-side wait exceeded its limit (decoupled look-back)");
+  if (e & DERR_BOUNDS) return fail(JFX_ERR_ARG, "a device-side bounds check failed");
+  return JFX_OK;
+}
+
+// Header shared by every entry point: error word + min/max scratch + readback.
+struct Common {
+  u32* err;
+  u64* mm;    // [4 * kMaxCols]
+  u64* words; // [8] values read back by the host
+};
+static void take_common(Arena& ar, Common& c) {
+  c.err = ar.take<u32>(64);
+  c.mm = ar.take<u64>(4 * kMaxCols);
+  c.words = ar.take<u64>(8);
+}
+
+template <typename K>
+__global__ void k_unpack(const K* sk, u64 n, int dtype, u32 flags, u64 tmin, void* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    store_raw(out, dtype, i, untransform_int(dtype, flags, (u64)sk[i] + tmin));
+}
+
+__global__ void k_gather_same(const void* src, int dt, const u32* idx, u64 n, void* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    store_raw(out, dt, i, load_raw(src, dt, idx[i]));
+}
+
+// ------------------------------------------------------------------ sort ---
+static void carve_sort(Arena& ar, u64 n, Common& c, SortBuffers& b) {
+  take_common(ar, c);
+  take_sort_buffers(ar, n, b);
+}
+
+// ---------------------------------------------------------------- lexsort ---
+static void carve_lexsort(Arena& ar, u64 n, Common& c, SortBuffers& b, u32** tmp) {
+  carve_sort(ar, n, c, b);
+  *tmp = ar.take<u32>(n ? n : 1);
+}
+
+// ---------------------------------------------------------------- groupby ---
+struct GroupBuffers {
+  void* sk;
+  u32* perm;
+  u32* warp_count;
+  u32* warp_base;
+  u32* partial;
+  u32* total;
+  u32* slot_gid;
+  u32* slot_started;
+  u64* slot_state;
+  u64 nwarps;
+};
+static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b, GroupBuffers& g) {
+  carve_sort(ar, n, c, b);
+  g.sk = ar.take<u64>(n ? n : 1);
+  g.perm = ar.take<u32>(n ? n : 1);
+  g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
+  g.warp_count = ar.take<u32>(g.nwarps + 1);
+  g.warp_base = ar.take<u32>(g.nwarps + 1);
+  g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
+  g.total = ar.take<u32>(4);
+  g.slot_gid = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_started = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_state = ar.take<u64>((u64)std::max(nvals, 1) * 4 * (2 * g.nwarps + 1));
+}
+
+// ------------------------------------------------------------------- join ---
+struct JoinPlan {
+  u64 magic;
+  int how;
+  int key64;
+  int dtype;
+  u32 flags;
+  u64 tmin;
+  u64 nl, nr, m;
+  const void* lkey;
+  const void* rkey;
+  void* skL;
+  void* skR;
+  u32* pL;
+  u32* pR;
+  u32* lo;
+  u32* cnt;
+  u64* off;
+};
+static_assert(sizeof(JoinPlan) <= sizeof(jfx_join_plan), "join plan does not fit");
+constexpr u64 kJoinMagic = 0x6a66786a6f696e31ull;
+
+struct JoinBuffers {
+  void *skL, *skR;
+  u32 *pL, *pR, *lo, *cnt;
+  u64 *off, *partial, *total;
+};
+static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
+  take_common(ar, c);
+  u64 nmax = std::max(nl, nr);
+  take_sort_buffers(ar, nmax, b);
+  j.skL = ar.take<u64>(nl ? nl : 1);
+  j.skR = ar.take<u64>(nr ? nr : 1);
+  j.pL = ar.take<u32>(nl ? nl : 1);
+  j.pR = ar.take<u32>(nr ? nr : 1);
+  j.lo = ar.take<u32>(nmax ? nmax : 1);
+  j.cnt = ar.take<u32>(nmax ? nmax : 1);
+  j.off = ar.take<u64>(nmax ? nmax : 1);
+  j.partial = ar.take<u64>(scan_partials_count(nmax));
+  j.total = ar.take<u64>(4);
+}
+
+// -------------------------------------------------------------- partition ---
+static void carve_partition(Arena& ar, u64 n, Common& c, SortBuffers& b) { carve_sort(ar, n, c, b); }
+
+static int check_n(int64_t n) {
+  if (n < 0) return fail(JFX_ERR_ARG, "negative row count %lld", (long long)n);
+  if (n > kMaxRows) return fail(JFX_ERR_CAPACITY, "%lld rows exceed the %lld-row limit", (long long)n, (long long)kMaxRows);
+  return JFX_OK;
+}
+
+}  // namespace jfx
+
+using namespace jfx;
+
+extern "C" {
+
+const char* jfx_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t jfx_launch_count(void) { return g_launches.load(); }
+
+int jfx_timing_enable(int enable) {
+  std::lock_guard<std::mutex> lk(g_timing.mu);
+  for (auto& r : g_timing.recs) {
+    g_timing.pool.push_back(r.start);
+    g_timing.pool.push_back(r.stop);
+  }
+  g_timing.recs.clear();
+  g_timing.on = enable != 0;
+  return JFX_OK;
+}
+
+int jfx_timing_read(double* total_ms, int64_t* launches, double* algo_bytes) {
+  std::lock_guard<std::mutex> lk(g_timing.mu);
+  double ms = 0, bytes = 0;
+  for (auto& r : g_timing.recs) {
+    JFX_CUDA(cudaEventSynchronize(r.stop));
+    float e = 0;
+    JFX_CUDA(cudaEventElapsedTime(&e, r.start, r.stop));
+    ms += e;
+    bytes += r.bytes;
+  }
+  if (total_ms) *total_ms = ms;
+  if (launches) *launches = (int64_t)g_timing.recs.size();
+  if (algo_bytes) *algo_bytes = bytes;
+  return JFX_OK;
+}
+int jfx_version(void) { return 1; }
+int jfx_max_rows(void) { return (int)kMaxRows; }
+
+size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2) {
+  Arena ar(nullptr, ~size_t(0));
+  Common c;
+  SortBuffers b;
+  u64 a = n1 > 0 ? (u64)n1 : 0, bn = n2 > 0 ? (u64)n2 : 0;
+  switch (kind) {
+    case JFX_WS_SORT: {
+      u32* tmp;
+      carve_lexsort(ar, a, c, b, &tmp);
+      break;
+    }
+    case JFX_WS_GROUPBY: {
+      GroupBuffers g;
+      carve_groupby(ar, a, kMaxVals, c, b, g);
+      break;
+    }
+    case JFX_WS_JOIN: {
+      JoinBuffers j;
+      carve_join(ar, a, bn, c, b, j);
+      break;
+    }
+    case JFX_WS_PARTITION:
+      carve_partition(ar, a, c, b);
+      break;
+    default:
+      return 0;
+  }
+  return ar.off + 256;
+}
+
+int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out, void* sorted_keys_out,
+             void* workspace, size_t workspace_bytes, void* stream) {
+  JFX_TRY(check_n(n));
+  if (!key || !perm_out) return fail(JFX_ERR_ARG, "null key or permutation pointer");
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  PackDesc pd;
+  JFX_TRY(build_pack(key, 1, CF_QUIRK, false, pd));
+  if (key->dtype == JFX_BOOL) return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  carve_sort(ar, (u64)n, c, b);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  KeyPlan kp;
+  kp.pack = pd;
+  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s));
+  RadixRequest rq;
+  rq.pack = kp.pack;
+  rq.total_bits = kp.total_bits;
+  rq.key64 = kp.total_bits > 32;
+  rq.reverse = !ascending;
+  rq.perm_out = (u32*)perm_out;
+  JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+  if (sorted_keys_out) {
+    const int g = grid_for((u64)n, 256);
+    if (dtype_is_float(key->dtype)) {
+      k_gather_same<<<g, 256, 0, s>>>(key->data, key->dtype, (const u32*)perm_out, (u64)n, sorted_keys_out), note_launch();
+    } else if (rq.key64) {
+      k_unpack<u64><<<g, 256, 0, s>>>((const u64*)rq.keys_result, (u64)n, key->dtype, CF_QUIRK, kp.pack.c[0].tmin, sorted_keys_out), note_launch();
+    } else {
+      k_unpack<u32><<<g, 256, 0, s>>>((const u32*)rq.keys_result, (u64)n, key->dtype, CF_QUIRK, kp.pack.c[0].tmin, sorted_keys_out), note_launch();
+    }
+    JFX_CUDA(cudaGetLastError());
+  }
+  u64* host = g_host.get();
+  JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+  return check_err_word((u32)host[0]);
+}
+
+int jfx_lexsort(const jfx_column* keys, int ncols, int64_t n, int32_t* perm_out, void* workspace,
+                size_t workspace_bytes, void* stream) {
+  JFX_TRY(check_n(n));
+  if (!keys || !perm_out) return fail(JFX_ERR_ARG, "null keys or permutation pointer");
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  PackDesc pd;
+  // one key: plain stable ascending argsort, `ascending` ignored (line 44-45)
+  JFX_TRY(build_pack(keys, ncols, 0u, ncols > 1, pd));
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  u32* tmp;
+  carve_lexsort(ar, (u64)n, c, b, &tmp);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  KeyPlan kp;
+  kp.pack = pd;
+  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s));
+  if (kp.total_bits <= 64) {
+    RadixRequest rq;
+    rq.pack = kp.pack;
+    rq.total_bits = kp.total_bits;
+    rq.key64 = kp.total_bits > 32;
+    rq.perm_out = (u32*)perm_out;
+    JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+  } else {
+    // LSD over groups of columns whose packed width fits 64 bits, last group
+    // first; later rounds read their columns through the current order.
+    int groups[kMaxCols + 1], ng = 0;
+    int end = pd.ncols;
+    while (end > 0) {
+      int bits = 0, start = end;
+      while (start > 0 && bits + kp.pack.c[start - 1].bits <= 64) {
+        bits += kp.pack.c[start - 1].bits;
+        --start;
+      }
+      groups[ng++] = start;
+      end = start;
+    }
+    // groups[r] = first column of round r; round r covers [groups[r], prev_end)
+    u32* bufs[2] = {(u32*)perm_out, tmp};
+    int prev_end = pd.ncols;
+    const u32* gather = nullptr;
+    for (int r = 0; r < ng; ++r) {
+      int start = groups[r];
+      RadixRequest rq;
+      memset(&rq.pack, 0, sizeof rq.pack);
+      rq.pack.ncols = prev_end - start;
+      int shift = 0;
+      for (int j = prev_end - 1; j >= start; --j) {
+        ColDesc cd = kp.pack.c[j];
+        cd.shift = shift;
+        shift += cd.bits;
+        rq.pack.c[j - start] = cd;
+      }
+      rq.total_bits = shift;
+      rq.key64 = shift > 32;
+      rq.gather_idx = gather;
+      u32* out = bufs[(ng - 1 - r) & 1];
+      rq.perm_out = out;
+      if (shift == 0) {
+        if (!gather) {
+          k_iota<<<grid_for((u64)n, 256), 256, 0, s>>>(out, (u64)n, 0), note_launch();
+        } else {
+          JFX_CUDA(cudaMemcpyAsync(out, gather, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+        }
+      } else {
+        JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+      }
+      gather = out;
+      prev_end = start;
+    }
+  }
+  u64* host = g_host.get();
+  JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+  return check_err_word((u32)host[0]);
+}
+
+int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, const jfx_agg_column* values,
+                int nvalues, void* const* unique_out, int64_t* num_groups, void* workspace, size_t workspace_bytes,
+                void* stream) {
+  JFX_TRY(check_n(n));
+  if (!keys || !num_groups) return fail(JFX_ERR_ARG, "null keys or num_groups pointer");
+  if (nvalues < 0 || nvalues > kMaxVals) return fail(JFX_ERR_ARG, "0..%d value columns supported", kMaxVals);
+  if (!multi_key && ncols != 1) return fail(JFX_ERR_ARG, "single-key groupby takes one key column");
+  *num_groups = 0;
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  PackDesc pd;
+  JFX_TRY(build_pack(keys, ncols, multi_key ? 0u : CF_QUIRK, false, pd));
+  if (!multi_key && keys[0].dtype == JFX_BOOL) return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
+  GroupArgs ga;
+  memset(&ga, 0, sizeof ga);
+  ga.nvals = nvalues;
+  for (int i = 0; i < nvalues; ++i) {
+    const jfx_agg_column& v = values[i];
+    ValDesc& d = ga.v[i];
+    if (!v.data) return fail(JFX_ERR_ARG, "value column %d has a null pointer", i);
+    if (dtype_size(v.dtype) == 0) return fail(JFX_ERR_DTYPE, "value column %d: unsupported dtype", i);
+    if (v.aggs & ~31u) return fail(JFX_ERR_ARG, "value column %d: unknown aggregation bits 0x%x", i, v.aggs);
+    d.ptr = v.data;
+    d.dtype = v.dtype;
+    d.kind = dtype_is_float(v.dtype) ? VK_F : dtype_is_signed_int(v.dtype) ? VK_I : VK_U;
+    d.aggs = v.aggs;
+    d.mean_dtype = v.mean_dtype;
+    d.count_dtype = v.count_dtype;
+    d.count_via_f32 = multi_key ? 1 : 0;
+    d.out_sum = v.out_sum;
+    d.out_mean = v.out_mean;
+    d.out_count = v.out_count;
+    d.out_min = v.out_min;
+    d.out_max = v.out_max;
+    if (((v.aggs & JFX_AGG_SUM) && !v.out_sum) || ((v.aggs & JFX_AGG_MEAN) && !v.out_mean) ||
+        ((v.aggs & JFX_AGG_COUNT) && !v.out_count) || ((v.aggs & JFX_AGG_MIN) && !v.out_min) ||
+        ((v.aggs & JFX_AGG_MAX) && !v.out_max))
+      return fail(JFX_ERR_ARG, "value column %d: missing output pointer", i);
+    if ((v.aggs & JFX_AGG_MEAN) && v.mean_dtype != JFX_F32 && v.mean_dtype != JFX_F64)
+      return fail(JFX_ERR_DTYPE, "value column %d: mean dtype must be float32 or float64", i);
+    if ((v.aggs & JFX_AGG_COUNT) && dtype_size(v.count_dtype) == 0)
+      return fail(JFX_ERR_DTYPE, "value column %d: bad count dtype", i);
+  }
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  GroupBuffers g;
+  carve_groupby(ar, (u64)n, nvalues, c, b, g);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  KeyPlan kp;
+  kp.pack = pd;
+  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s));
+  if (kp.total_bits > 64)
+    return fail(JFX_ERR_CAPACITY, "group keys need %d packed bits; at most 64 are supported", kp.total_bits);
+  RadixRequest rq;
+  rq.pack = kp.pack;
+  rq.total_bits = kp.total_bits;
+  rq.key64 = kp.total_bits > 32;
+  rq.perm_out = g.perm;
+  rq.keys_out = g.sk;
+  JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+
+  ga.skeys = g.sk;
+  ga.perm = g.perm;
+  ga.n = (u64)n;
+  ga.warp_count = g.warp_count;
+  ga.warp_base = g.warp_base;
+  ga.pack = kp.pack;
+  for (int j = 0; j < ncols; ++j) ga.uniq_out[j] = unique_out ? unique_out[j] : nullptr;
+  ga.slot_gid = g.slot_gid;
+  ga.slot_started = g.slot_started;
+  ga.slot_state = g.slot_state;
+  ga.nslots = 2 * g.nwarps;
+  const unsigned blocks = (unsigned)((g.nwarps * 32 + 255) / 256);
+  if (rq.key64) k_group_count<u64><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  else k_group_count<u32><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
+  JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
+  if (rq.key64) k_group_reduce<u64><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  else k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  k_group_fixup<<<(unsigned)((ga.nslots + 255) / 256), 256, 0, s>>>(ga), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  u64* host = g_host.get();
+  JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaMemcpyAsync(host + 1, g.total, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  JFX_TRY(check_err_word((u32)host[0]));
+  *num_groups = (int64_t)(u32)host[1];
+  return JFX_OK;
+}
+
+int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* right_key, int64_t nr, int how,
+                     jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
+                     void* stream) {
+  JFX_TRY(check_n(nl));
+  JFX_TRY(check_n(nr));
+  if (!left_key || !right_key || !plan_out || !num_out) return fail(JFX_ERR_ARG, "null argument");
+  if (left_key->dtype != right_key->dtype)
+    return fail(JFX_ERR_DTYPE, "join keys must share a dtype (got %d and %d)", left_key->dtype, right_key->dtype);
+  if (left_key->dtype == JFX_BOOL) return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
+  if (how != JFX_JOIN_INNER && how != JFX_JOIN_LEFT && how != JFX_JOIN_RIGHT)
+    return fail(JFX_ERR_ARG, "join kind %d is not supported by this entry point", how);
+  cudaStream_t s = as_stream(stream);
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  JoinBuffers j;
+  carve_join(ar, (u64)nl, (u64)nr, c, b, j);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  PackDesc pl, pr;
+  JFX_TRY(build_pack(left_key, 1, CF_QUIRK, false, pl));
+  JFX_TRY(build_pack(right_key, 1, CF_QUIRK, false, pr));
+  // shared packing: min and max over both sides
+  JFX_TRY(launch_minmax(pl, (u64)nl, c.mm, s));
+  JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2, s));
+  u64* host = g_host.get();
+  JFX_TRY(read_back(c.mm, 4 * sizeof(u64), host, s));
+  u64 mn = std::min(host[0], host[2]), mx = 0;
+  if (nl) mx = std::max(mx, host[1]);
+  if (nr) mx = std::max(mx, host[3]);
+  if (!nl && !nr) mn = 0;
+  const int bits = bit_length(mx - mn);
+  pl.c[0].tmin = pr.c[0].tmin = mn;
+  pl.c[0].bits = pr.c[0].bits = bits;
+  pl.c[0].shift = pr.c[0].shift = 0;
+  const bool key64 = bits > 32;
+  if (nl) {
+    RadixRequest rq;
+    rq.pack = pl;
+    rq.total_bits = bits;
+    rq.key64 = key64;
+    rq.perm_out = j.pL;
+    rq.keys_out = j.skL;
+    JFX_TRY(radix_sort(rq, (u64)nl, b, c.err, s));
+  }
+  if (nr) {
+    RadixRequest rq;
+    rq.pack = pr;
+    rq.total_bits = bits;
+    rq.key64 = key64;
+    rq.perm_out = j.pR;
+    rq.keys_out = j.skR;
+    JFX_TRY(radix_sort(rq, (u64)nr, b, c.err, s));
+  }
+  const int nan_key = dtype_is_float(left_key->dtype);
+  const u64 nant = left_key->dtype == JFX_F32 ? (u64)kF32NanT : kF64NanT;
+  const u64 nan_packed = nant - mn;
+  // count: A = the side whose rows drive the output
+  const bool swap = how == JFX_JOIN_RIGHT;
+  const u64 na = swap ? nr : nl, nb = swap ? nl : nr;
+  const void* A = swap ? j.skR : j.skL;
+  const void* B = swap ? j.skL : j.skR;
+  u64 m = 0;
+  if (na && nb) {
+    const unsigned blocks = (unsigned)((na + kJoinTile - 1) / kJoinTile);
+    if (key64)
+      k_join_count<u64><<<blocks, kJoinThreads, 0, s>>>((const u64*)A, na, (const u64*)B, nb, j.lo, j.cnt, nan_key, (u64)nan_packed), note_launch();
+    else
+      k_join_count<u32><<<blocks, kJoinThreads, 0, s>>>((const u32*)A, na, (const u32*)B, nb, j.lo, j.cnt, nan_key, (u32)nan_packed), note_launch();
+    JFX_CUDA(cudaGetLastError());
+  } else if (na) {
+    JFX_CUDA(cudaMemsetAsync(j.cnt, 0, na * sizeof(u32), s));
+    JFX_CUDA(cudaMemsetAsync(j.lo, 0, na * sizeof(u32), s));
+  }
+  if (how == JFX_JOIN_INNER) {
+    if (na && nb) {
+      JFX_TRY(device_exclusive_scan<u64>(j.cnt, na, j.off, j.total, j.partial, s));
+      JFX_CUDA(cudaMemcpyAsync(host + 1, j.total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+    } else {
+      host[1] = 0;
+    }
+  }
+  JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  JFX_TRY(check_err_word((u32)host[0]));
+  if (how == JFX_JOIN_INNER) {
+    m = (na && nb) ? host[1] : 0;
+    if (m > (u64)0x7fffffffull) return fail(JFX_ERR_CAPACITY, "inner join produces %llu rows; at most 2^31-1 are supported", m);
+  } else {
+    m = na;
+  }
+  JoinPlan* jp = (JoinPlan*)plan_out;
+  memset(plan_out, 0, sizeof *plan_out);
+  jp->magic = kJoinMagic;
+  jp->how = how;
+  jp->key64 = key64;
+  jp->dtype = left_key->dtype;
+  jp->flags = CF_QUIRK;
+  jp->tmin = mn;
+  jp->nl = (u64)nl;
+  jp->nr = (u64)nr;
+  jp->m = m;
+  jp->lkey = left_key->data;
+  jp->rkey = right_key->data;
+  jp->skL = j.skL;
+  jp->skR = j.skR;
+  jp->pL = j.pL;
+  jp->pR = j.pR;
+  jp->lo = j.lo;
+  jp->cnt = j.cnt;
+  jp->off = j.off;
+  *num_out = (int64_t)m;
+  return JFX_OK;
+}
+
+int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out, void* keys_out,
+                    void* stream) {
+  if (!plan) return fail(JFX_ERR_ARG, "null plan");
+  const JoinPlan* jp = (const JoinPlan*)plan;
+  if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
+  if (jp->m == 0) return JFX_OK;
+  if (!left_idx_out || !right_idx_out) return fail(JFX_ERR_ARG, "null index output");
+  cudaStream_t s = as_stream(stream);
+  const bool swap = jp->how == JFX_JOIN_RIGHT;
+  JoinKeyOut ko;
+  ko.keys_out = keys_out;
+  ko.dtype = jp->dtype;
+  ko.flags = jp->flags;
+  ko.tmin = jp->tmin;
+  ko.orig = swap ? jp->rkey : jp->lkey;
+  const u64 na = swap ? jp->nr : jp->nl;
+  const void* skA = swap ? jp->skR : jp->skL;
+  const u32* pA = swap ? jp->pR : jp->pL;
+  const u32* pB = swap ? jp->pL : jp->pR;
+  int32_t* a_out = swap ? right_idx_out : left_idx_out;
+  int32_t* b_out = swap ? left_idx_out : right_idx_out;
+  if (jp->how == JFX_JOIN_INNER) {
+    const unsigned blocks = (unsigned)((jp->m + kJoinTile - 1) / kJoinTile);
+    if (jp->key64)
+      k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko), note_launch();
+    else
+      k_join_expand_inner<u32><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko), note_launch();
+  } else {
+    const int g = grid_for(na, 256);
+    if (jp->key64)
+      k_join_expand_first<u64><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u64*)skA, a_out, b_out, ko), note_launch();
+    else
+      k_join_expand_first<u32><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u32*)skA, a_out, b_out, ko), note_launch();
+  }
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+int jfx_gather(const void* src, int32_t src_dtype, int64_t n_src, const int32_t* idx, int64_t n, void* out,
+               int32_t out_dtype, void* stream) {
+  if (n < 0 || n_src < 0) return fail(JFX_ERR_ARG, "negative count");
+  if (n == 0) return JFX_OK;
+  if (!idx || !out || (!src && n_src)) return fail(JFX_ERR_ARG, "null pointer");
+  if (dtype_size(src_dtype) == 0 || dtype_size(out_dtype) == 0) return fail(JFX_ERR_DTYPE, "unsupported dtype");
+  cudaStream_t s = as_stream(stream);
+  k_gather<<<grid_for((u64)n, 256), 256, 0, s>>>(src, src_dtype, (u64)n_src, idx, (u64)n, out, out_dtype), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+int jfx_hash_columns(const jfx_column* keys, int ncols, int64_t n, uint32_t* hash_out, void* stream) {
+  if (n < 0) return fail(JFX_ERR_ARG, "negative count");
+  if (!hash_out) return fail(JFX_ERR_ARG, "null output");
+  PackDesc pd;
+  JFX_TRY(build_pack(keys, ncols, 0u, false, pd));
+  if (ncols == 1 && keys[0].dtype == JFX_F64)
+    return fail(JFX_ERR_DTYPE, "a single float64 key hashes to two words per row in the reference; not a row hash");
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  k_hash<<<grid_for((u64)n, 256), 256, 0, s>>>(pd, (u64)n, hash_out), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_partitions, int32_t* targets_out,
+                       int32_t* perm_out, int64_t* offsets_out, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+  JFX_TRY(check_n(n));
+  if (num_partitions < 1 || num_partitions > 2048) return fail(JFX_ERR_ARG, "num_partitions must be in [1, 2048]");
+  if (!perm_out || !offsets_out) return fail(JFX_ERR_ARG, "null output");
+  PackDesc pd;
+  JFX_TRY(build_pack(keys, ncols, 0u, false, pd));
+  if (ncols == 1 && keys[0].dtype == JFX_F64)
+    return fail(JFX_ERR_DTYPE, "a single float64 key hashes to two words per row in the reference; not a row hash");
+  cudaStream_t s = as_stream(stream);
+  if (n == 0) {
+    JFX_CUDA(cudaMemsetAsync(offsets_out, 0, (num_partitions + 1) * sizeof(int64_t), s));
+    return JFX_OK;
+  }
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  carve_partition(ar, (u64)n, c, b);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  RadixRequest rq;
+  rq.pack = pd;
+  rq.key_mode = KEY_HASH;
+  rq.digit_mode = DIG_MOD;
+  rq.modulus = (u32)num_partitions;
+  rq.key64 = false;
+  rq.targets = (u32*)targets_out;
+  rq.perm_out = (u32*)perm_out;
+  JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+  k_offsets_from_base<<<1, 256, 0, s>>>(b.base, num_partitions, (u64)n, offsets_out), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  u64* host = g_host.get();
+  JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+  return check_err_word((u32)host[0]);
+}
+
+}  // extern "C"

@@ -1,0 +1,555 @@
+// groupby.cuh -- sort-based groupby: segment-boundary flags over the sorted
+// packed keys, then a warp-level segmented reduction of each value column
+// gathered through the sort permutation.
+//
+// Replaces SortBasedGroupBy.groupby_aggregate (parallel_algorithms.py:733-803,
+// boundary flags :767-770, host group count :772, nonzero/cumsum :773-777,
+// jax.ops.segment_* :626-660) and groupby_aggregate_multi_column (:662-731,
+// _scatter_group_aggregate :1212-1228).
+//
+// Every warp owns 32*IPT consecutive sorted rows.  A group that starts and
+// ends inside one warp is written by that warp.  A group that crosses a warp
+// boundary leaves one partial record per warp it touches (at most two per
+// warp); k_group_fixup combines those records in row order.  Float sums are
+// accumulated in float64 and rounded once, so results are deterministic.
+#pragma once
+
+#include "radix.cuh"
+
+namespace jfx {
+
+constexpr int kMaxVals = 16;
+constexpr int kGroupIPT = 16;
+constexpr u32 kEmptySlot = 0xffffffffu;
+
+enum : int { VK_F = 0, VK_I = 1, VK_U = 2 };
+
+struct ValDesc {
+  const void* ptr;
+  int dtype;
+  int kind;
+  u32 aggs;
+  int mean_dtype;
+  int count_dtype;
+  int count_via_f32;  // multi-key mean divides by a float32 count
+  void* out_sum;
+  void* out_mean;
+  void* out_count;
+  void* out_min;
+  void* out_max;
+};
+
+struct GroupArgs {
+  const void* skeys;  // sorted packed keys (K)
+  const u32* perm;    // sorted row ids
+  u64 n;
+  u32* warp_count;    // per-warp number of group starts (k_group_count)
+  const u32* warp_base;  // exclusive scan of warp_count
+  PackDesc pack;
+  void* uniq_out[kMaxCols];
+  int nvals;
+  ValDesc v[kMaxVals];
+  u32* slot_gid;      // [2 * warps]
+  u32* slot_started;  // [2 * warps]
+  u64* slot_state;    // [nvals][4][2 * warps]: sum, min, max, count
+  u64 nslots;
+};
+
+// NaN test on the packed key: a float key column holding the canonical NaN.
+template <typename K>
+__device__ __forceinline__ bool packed_has_nan(const PackDesc& pd, K k) {
+  if (!pd.nan_cols) return false;
+  for (int j = 0; j < pd.ncols; ++j) {
+    if (!((pd.nan_cols >> j) & 1)) continue;
+    const ColDesc& c = pd.c[j];
+    const u64 nant = c.dtype == JFX_F32 ? (u64)kF32NanT : kF64NanT;
+    if (c.bits == 0) {
+      if (c.tmin == nant) return true;
+      continue;
+    }
+    const u64 field = ((u64)k >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull));
+    if (field + c.tmin == nant) return true;
+  }
+  return false;
+}
+
+template <typename K>
+__device__ __forceinline__ bool row_flag(const GroupArgs& a, const K* sk, u64 row) {
+  const K k = sk[row];
+  if (row == 0) return true;
+  return k != sk[row - 1] || packed_has_nan<K>(a.pack, k);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_group_count(GroupArgs a, u64 nwarps) {
+  const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nwarps) return;
+  const K* sk = (const K*)a.skeys;
+  const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
+  u32 cnt = 0;
+#pragma unroll 4
+  for (int s = 0; s < kGroupIPT; ++s) {
+    const u64 row = wbeg + (u64)s * 32 + lane;
+    const bool f = row < wend && row_flag<K>(a, sk, row);
+    cnt += __popc(__ballot_sync(0xffffffffu, f));
+  }
+  if (lane == 0) a.warp_count[w] = cnt;
+}
+
+// ---- per-kind partial state: sum, min, max (64-bit words) and row count ----
+template <int KIND>
+struct Agg {
+  u64 sum, mn, mx;
+  u32 cnt;
+};
+
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_identity() {
+  Agg<KIND> s;
+  s.cnt = 0;
+  if (KIND == VK_F) {
+    s.sum = __double_as_longlong(0.0);
+    s.mn = __double_as_longlong(__longlong_as_double(0x7ff0000000000000ll));   // +inf
+    s.mx = __double_as_longlong(__longlong_as_double((long long)0xfff0000000000000ull));  // -inf
+  } else if (KIND == VK_I) {
+    s.sum = 0;
+    s.mn = 0x7fffffffffffffffull;
+    s.mx = 0x8000000000000000ull;
+  } else {
+    s.sum = 0;
+    s.mn = ~0ull;
+    s.mx = 0ull;
+  }
+  return s;
+}
+
+// a precedes b in row order; ties keep a.
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_combine(const Agg<KIND>& a, const Agg<KIND>& b) {
+  Agg<KIND> r;
+  r.cnt = a.cnt + b.cnt;
+  if (KIND == VK_F) {
+    const double as = __longlong_as_double(a.sum), bs = __longlong_as_double(b.sum);
+    r.sum = __double_as_longlong(as + bs);
+    const double an = __longlong_as_double(a.mn), bn = __longlong_as_double(b.mn);
+    const double ax = __longlong_as_double(a.mx), bx = __longlong_as_double(b.mx);
+    // lax.min / lax.max propagate NaN
+    r.mn = (an != an) ? a.mn : (bn != bn) ? b.mn : (bn < an ? b.mn : a.mn);
+    r.mx = (ax != ax) ? a.mx : (bx != bx) ? b.mx : (bx > ax ? b.mx : a.mx);
+  } else if (KIND == VK_I) {
+    r.sum = a.sum + b.sum;
+    r.mn = ((long long)b.mn < (long long)a.mn) ? b.mn : a.mn;
+    r.mx = ((long long)b.mx > (long long)a.mx) ? b.mx : a.mx;
+  } else {
+    r.sum = a.sum + b.sum;
+    r.mn = b.mn < a.mn ? b.mn : a.mn;
+    r.mx = b.mx > a.mx ? b.mx : a.mx;
+  }
+  return r;
+}
+
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_of(const ValDesc& v, u64 row) {
+  Agg<KIND> s;
+  s.cnt = 1;
+  u64 w;
+  if (KIND == VK_F) {
+    double x = v.dtype == JFX_F32 ? (double)__ldg((const float*)v.ptr + row) : __ldg((const double*)v.ptr + row);
+    w = __double_as_longlong(x);
+  } else if (KIND == VK_I) {
+    long long x;
+    switch (v.dtype) {
+      case JFX_I8: x = ((const signed char*)v.ptr)[row]; break;
+      case JFX_I16: x = ((const short*)v.ptr)[row]; break;
+      case JFX_I32: x = __ldg((const int*)v.ptr + row); break;
+      default: x = __ldg((const long long*)v.ptr + row); break;
+    }
+    w = (u64)x;
+  } else {
+    switch (v.dtype) {
+      case JFX_U8: case JFX_BOOL: w = ((const unsigned char*)v.ptr)[row]; break;
+      case JFX_U16: w = ((const unsigned short*)v.ptr)[row]; break;
+      case JFX_U32: w = __ldg((const unsigned*)v.ptr + row); break;
+      default: w = __ldg((const u64*)v.ptr + row); break;
+    }
+  }
+  s.sum = s.mn = s.mx = w;
+  return s;
+}
+
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_shfl_up(const Agg<KIND>& s, int o) {
+  Agg<KIND> r;
+  r.sum = __shfl_up_sync(0xffffffffu, s.sum, o);
+  r.mn = __shfl_up_sync(0xffffffffu, s.mn, o);
+  r.mx = __shfl_up_sync(0xffffffffu, s.mx, o);
+  r.cnt = __shfl_up_sync(0xffffffffu, s.cnt, o);
+  return r;
+}
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_shfl(const Agg<KIND>& s, int src) {
+  Agg<KIND> r;
+  r.sum = __shfl_sync(0xffffffffu, s.sum, src);
+  r.mn = __shfl_sync(0xffffffffu, s.mn, src);
+  r.mx = __shfl_sync(0xffffffffu, s.mx, src);
+  r.cnt = __shfl_sync(0xffffffffu, s.cnt, src);
+  return r;
+}
+
+__device__ __forceinline__ void store_float(void* base, int dtype, u64 i, double x) {
+  if (dtype == JFX_F32) ((float*)base)[i] = (float)x;
+  else ((double*)base)[i] = x;
+}
+
+// Value of the group's sum in the value dtype, as a double (for the mean).
+template <int KIND>
+__device__ __forceinline__ double sum_in_value_dtype(const ValDesc& v, u64 sum) {
+  if (KIND == VK_F) {
+    double s = __longlong_as_double(sum);
+    return v.dtype == JFX_F32 ? (double)(float)s : s;
+  }
+  // integer sums wrap in the value dtype
+  const int bits = dtype_bits(v.dtype);
+  if (KIND == VK_I) {
+    long long x = bits >= 64 ? (long long)sum : ((long long)(sum << (64 - bits)) >> (64 - bits));
+    return (double)x;
+  }
+  u64 x = bits >= 64 ? sum : (sum & ((1ull << bits) - 1ull));
+  return (double)x;
+}
+
+template <int KIND>
+__device__ __forceinline__ void agg_finalize(const ValDesc& v, u64 g, const Agg<KIND>& s) {
+  if (v.aggs & JFX_AGG_SUM) {
+    if (KIND == VK_F) store_float(v.out_sum, v.dtype, g, __longlong_as_double(s.sum));
+    else store_raw(v.out_sum, v.dtype, g, s.sum);
+  }
+  if (v.aggs & JFX_AGG_MEAN) {
+    double c = v.count_via_f32 ? (double)(float)s.cnt : (double)s.cnt;
+    if (v.mean_dtype == JFX_F32) {
+      // float32 arithmetic: float(sum in value dtype) / float(count)
+      float num;
+      if (KIND == VK_F) num = (float)sum_in_value_dtype<KIND>(v, s.sum);
+      else if (KIND == VK_I) {
+        const int bits = dtype_bits(v.dtype);
+        long long x = bits >= 64 ? (long long)s.sum : ((long long)(s.sum << (64 - bits)) >> (64 - bits));
+        num = (float)x;
+      } else {
+        const int bits = dtype_bits(v.dtype);
+        u64 x = bits >= 64 ? s.sum : (s.sum & ((1ull << bits) - 1ull));
+        num = (float)x;
+      }
+      ((float*)v.out_mean)[g] = num / (float)c;
+    } else {
+      double num;
+      if (KIND == VK_F) num = sum_in_value_dtype<KIND>(v, s.sum);
+      else if (KIND == VK_I) {
+        const int bits = dtype_bits(v.dtype);
+        long long x = bits >= 64 ? (long long)s.sum : ((long long)(s.sum << (64 - bits)) >> (64 - bits));
+        num = (double)x;
+      } else {
+        const int bits = dtype_bits(v.dtype);
+        u64 x = bits >= 64 ? s.sum : (s.sum & ((1ull << bits) - 1ull));
+        num = (double)x;
+      }
+      ((double*)v.out_mean)[g] = num / c;
+    }
+  }
+  if (v.aggs & JFX_AGG_COUNT) {
+    switch (v.count_dtype) {
+      case JFX_F32: ((float*)v.out_count)[g] = (float)s.cnt; break;
+      case JFX_F64: ((double*)v.out_count)[g] = (double)s.cnt; break;
+      default: store_raw(v.out_count, v.count_dtype, g, (u64)s.cnt); break;
+    }
+  }
+  if (v.aggs & JFX_AGG_MIN) {
+    if (KIND == VK_F) store_float(v.out_min, v.dtype, g, __longlong_as_double(s.mn));
+    else store_raw(v.out_min, v.dtype, g, s.mn);
+  }
+  if (v.aggs & JFX_AGG_MAX) {
+    if (KIND == VK_F) store_float(v.out_max, v.dtype, g, __longlong_as_double(s.mx));
+    else store_raw(v.out_max, v.dtype, g, s.mx);
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ void slot_store(const GroupArgs& a, int c, u64 slot, u32 gid, u32 started,
+                                           const Agg<KIND>& s) {
+  u64* st = a.slot_state + (u64)c * 4 * a.nslots;
+  st[slot] = s.sum;
+  st[a.nslots + slot] = s.mn;
+  st[2 * a.nslots + slot] = s.mx;
+  st[3 * a.nslots + slot] = s.cnt;
+  if (c == 0) {
+    a.slot_gid[slot] = gid;
+    a.slot_started[slot] = started;
+  }
+}
+
+// Segmented reduction of one value column over the warp's rows.
+template <int KIND>
+__device__ __forceinline__ void reduce_column(const GroupArgs& a, int c, const u32 (&fm)[kGroupIPT],
+                                              const u32 (&pr)[kGroupIPT], u64 w, u64 wbeg, u64 wend,
+                                              u32 gbase, bool closed_end) {
+  const ValDesc& v = a.v[c];
+  const int lane = threadIdx.x & 31;
+  const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
+  const u32 le = (2u << lane) - 1u;  // lanemask_le
+  Agg<KIND> open = agg_identity<KIND>();
+  bool open_valid = false, open_started = false;
+  u32 open_gid = 0, gcount = 0;
+#pragma unroll
+  for (int s = 0; s < kGroupIPT; ++s) {
+    const u64 step0 = wbeg + (u64)s * 32;
+    if (step0 >= wend) break;
+    const u64 row = step0 + lane;
+    const bool valid = row < wend;
+    const u32 f = fm[s];
+    Agg<KIND> st = agg_identity<KIND>();
+    if (valid) {
+      if (need_vals) st = agg_of<KIND>(v, pr[s]);
+      else st.cnt = 1;
+    }
+    const u32 hb = f & le;
+    const int h = hb ? 31 - __clz(hb) : -1;
+    const int lo = h < 0 ? 0 : h;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      Agg<KIND> up = agg_shfl_up<KIND>(st, o);
+      if (lane - o >= lo) st = agg_combine<KIND>(up, st);
+    }
+    Agg<KIND> full = st;
+    bool started = h >= 0;
+    if (h < 0) {
+      if (open_valid) full = agg_combine<KIND>(open, st);
+      started = open_valid && open_started;
+    }
+    const u32 gid = gbase + gcount + __popc(f & le) - 1u;
+    const bool next_in_step = valid && lane < 31 && (row + 1 < wend);
+    const bool last_in_step = valid && !next_in_step;
+    bool closes;
+    if (next_in_step) closes = (f >> (lane + 1)) & 1u;
+    else if (row + 1 < wend) closes = (s + 1 < kGroupIPT) ? (fm[s + 1] & 1u) : true;
+    else closes = closed_end;
+    if (valid && (closes && (next_in_step || last_in_step))) {
+      if (started) agg_finalize<KIND>(v, gid, full);
+      else slot_store<KIND>(a, c, 2 * w, gid, 0u, full);  // the warp's first group, begun earlier
+    }
+    const u32 vm = __ballot_sync(0xffffffffu, valid);
+    const int last = 31 - __clz(vm);
+    const bool lc = __shfl_sync(0xffffffffu, closes, last);
+    Agg<KIND> lf = agg_shfl<KIND>(full, last);
+    const bool ls = __shfl_sync(0xffffffffu, started, last);
+    const u32 lg = __shfl_sync(0xffffffffu, gid, last);
+    if (lc) {
+      open_valid = false;
+    } else {
+      open = lf;
+      open_valid = true;
+      open_started = ls;
+      open_gid = lg;
+    }
+    gcount += __popc(f);
+  }
+  if (open_valid && lane == 0) slot_store<KIND>(a, c, 2 * w + 1, open_gid, open_started ? 1u : 0u, open);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_group_reduce(GroupArgs a, u64 nwarps) {
+  const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nwarps) return;
+  const K* sk = (const K*)a.skeys;
+  const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
+  const u32 gbase = a.warp_base[w];
+  const u32 le = (2u << lane) - 1u;
+  u32 fm[kGroupIPT], pr[kGroupIPT];
+  u32 gcount = 0;
+#pragma unroll
+  for (int s = 0; s < kGroupIPT; ++s) {
+    const u64 row = wbeg + (u64)s * 32 + lane;
+    const bool valid = row < wend;
+    K k = 0, kp = 0;
+    if (valid) k = sk[row];
+    kp = __shfl_up_sync(0xffffffffu, k, 1);
+    if (lane == 0 && valid && row > 0) kp = sk[row - 1];
+    const bool f = valid && (row == 0 || k != kp || packed_has_nan<K>(a.pack, k));
+    fm[s] = __ballot_sync(0xffffffffu, f);
+    pr[s] = valid ? a.perm[row] : 0u;
+    if (f) {
+      // unique key columns of the new group
+      const u32 gid = gbase + gcount + __popc(fm[s] & le) - 1u;
+      for (int j = 0; j < a.pack.ncols; ++j) {
+        const ColDesc& c = a.pack.c[j];
+        if (!a.uniq_out[j]) continue;
+        if (dtype_is_float(c.dtype)) {
+          store_raw(a.uniq_out[j], c.dtype, gid, load_raw(c.ptr, c.dtype, pr[s]));
+        } else {
+          const u64 field = c.bits ? (((u64)k >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull))) : 0ull;
+          store_raw(a.uniq_out[j], c.dtype, gid, untransform_int(c.dtype, c.flags, field + c.tmin));
+        }
+      }
+    }
+    gcount += __popc(fm[s]);
+  }
+  bool closed_end = true;
+  if (wend < a.n) closed_end = row_flag<K>(a, sk, wend);
+  for (int c = 0; c < a.nvals; ++c) {
+    switch (a.v[c].kind) {
+      case VK_F: reduce_column<VK_F>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
+      case VK_I: reduce_column<VK_I>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
+      default: reduce_column<VK_U>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
+    }
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> slot_load(const GroupArgs& a, int c, u64 i) {
+  const u64* st = a.slot_state + (u64)c * 4 * a.nslots;
+  Agg<KIND> s;
+  s.sum = st[i];
+  s.mn = st[a.nslots + i];
+  s.mx = st[2 * a.nslots + i];
+  s.cnt = (u32)st[3 * a.nslots + i];
+  return s;
+}
+
+template <int KIND>
+__device__ void fixup_column(const GroupArgs& a, int c, u64 i, u32 g) {
+  Agg<KIND> s = slot_load<KIND>(a, c, i);
+  for (u64 j = i + 1; j < a.nslots; ++j) {
+    const u32 gj = a.slot_gid[j];
+    if (gj == kEmptySlot) continue;
+    if (gj != g || a.slot_started[j]) break;
+    s = agg_combine<KIND>(s, slot_load<KIND>(a, c, j));
+  }
+  agg_finalize<KIND>(a.v[c], g, s);
+}
+
+// One thread per partial record; the record holding the group's first row
+// combines the group's records in row order and writes the result.
+__global__ void __launch_bounds__(256) k_group_fixup(GroupArgs a) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nslots) return;
+  const u32 g = a.slot_gid[i];
+  if (g == kEmptySlot || !a.slot_started[i]) return;
+  for (int c = 0; c < a.nvals; ++c) {
+    switch (a.v[c].kind) {
+      case VK_F: fixup_column<VK_F>(a, c, i, g); break;
+      case VK_I: fixup_column<VK_I>(a, c, i, g); break;
+      default: fixup_column<VK_U>(a, c, i, g); break;
+    }
+  }
+}
+
+// ---------------------------------------------------- device-wide scan ---
+// Exclusive scan of m u32 values into T (u32 or u64); *total = sum.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_reduce(const u32* in, u64 m, T* partial) {
+  __shared__ T sh[32];
+  const u64 base = (u64)blockIdx.x * 4096;
+  T s = 0;
+  for (int k = 0; k < 4; ++k) {
+    u64 i = base + (u64)k * 1024 + threadIdx.x;
+    if (i < m) s += (T)in[i];
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    T x = sh[threadIdx.x];
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = x;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_partials(T* partial, u64 nb, T* total) {
+  __shared__ T sh[32];
+  T carry = 0;
+  for (u64 b0 = 0; b0 < nb; b0 += 1024) {
+    u64 i = b0 + threadIdx.x;
+    T x = i < nb ? partial[i] : 0;
+    T inc = x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      T wv = sh[lane];
+      T wi = wv;
+      for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      sh[lane] = wi - wv;
+    }
+    __syncthreads();
+    T ex = inc - x + sh[warp] + carry;
+    if (i < nb) partial[i] = ex;
+    __syncthreads();
+    if (threadIdx.x == 1023) sh[0] = ex + x;
+    __syncthreads();
+    carry = sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_apply(const u32* in, u64 m, const T* partial, T* out) {
+  __shared__ T sh[32];
+  const u64 base = (u64)blockIdx.x * 4096;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // each thread: 4 consecutive items
+  T v[4], s = 0;
+  for (int k = 0; k < 4; ++k) {
+    u64 i = base + (u64)threadIdx.x * 4 + k;
+    v[k] = i < m ? (T)in[i] : 0;
+    s += v[k];
+  }
+  T inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) sh[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T wv = sh[lane];
+    T wi = wv;
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    sh[lane] = wi - wv;
+  }
+  __syncthreads();
+  T ex = inc - s + sh[warp] + partial[blockIdx.x];
+  for (int k = 0; k < 4; ++k) {
+    u64 i = base + (u64)threadIdx.x * 4 + k;
+    if (i < m) out[i] = ex;
+    ex += v[k];
+  }
+}
+
+template <typename T>
+inline int device_exclusive_scan(const u32* in, u64 m, T* out, T* total, T* partial, cudaStream_t s) {
+  u64 nb = (m + 4095) / 4096;
+  if (nb == 0) {
+    JFX_CUDA(cudaMemsetAsync(total, 0, sizeof(T), s));
+    return JFX_OK;
+  }
+  k_scan_reduce<T><<<(unsigned)nb, 1024, 0, s>>>(in, m, partial), note_launch();
+  k_scan_partials<T><<<1, 1024, 0, s>>>(partial, nb, total), note_launch();
+  k_scan_apply<T><<<(unsigned)nb, 1024, 0, s>>>(in, m, partial, out), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+inline u64 scan_partials_count(u64 m) { return (m + 4095) / 4096 + 1; }
+
+}  // namespace jfx

@@ -1,0 +1,206 @@
+// join.cuh -- sort-merge join over the two sorted packed key runs.
+//
+// Replaces ParallelSortMergeJoin.join (parallel_algorithms.py:938-1075).  The
+// reference finds inner matches with an nL x nR broadcast matrix
+// (:989-994); here both sides are radix sorted with one shared key packing,
+// a count pass finds, for every sorted left row, its equal-key run in the
+// sorted right side (binary search inside a shared-memory window of the right
+// run that the CTA's left tile can reach), an exclusive scan turns counts into
+// output offsets, and an expand pass writes the pairs with a load-balanced
+// search of the offsets.  Pair order is the matrix's row-major order:
+// (key, left row, right row).  left/right joins keep the first match
+// (searchsorted, :1013-1034).
+#pragma once
+
+#include "groupby.cuh"
+
+namespace jfx {
+
+constexpr int kJoinThreads = 256, kJoinIPT = 8, kJoinTile = kJoinThreads * kJoinIPT;
+
+template <typename K>
+__device__ __forceinline__ u64 lower_bound_g(const K* a, u64 lo, u64 hi, K x) {
+  while (lo < hi) {
+    u64 mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+template <typename K>
+__device__ __forceinline__ u64 upper_bound_g(const K* a, u64 lo, u64 hi, K x) {
+  while (lo < hi) {
+    u64 mid = (lo + hi) >> 1;
+    if (a[mid] <= x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// For each sorted A row: lo = first B position with key >= A[i], cnt = number
+// of B keys equal to A[i] (0 for a NaN key, which equals nothing).
+template <typename K>
+__global__ void __launch_bounds__(kJoinThreads) k_join_count(const K* A, u64 na, const K* B, u64 nb,
+                                                            u32* lo_out, u32* cnt_out, int nan_key,
+                                                            K nan_packed) {
+  constexpr int CAP = (32 * 1024) / sizeof(K);
+  __shared__ K win[CAP];
+  __shared__ u64 wlo_s, whi_s;
+  const u64 a0 = (u64)blockIdx.x * kJoinTile;
+  const u64 a1 = min(na, a0 + kJoinTile);
+  if (threadIdx.x == 0) {
+    wlo_s = lower_bound_g<K>(B, 0, nb, A[a0]);
+    whi_s = upper_bound_g<K>(B, wlo_s, nb, A[a1 - 1]);
+  }
+  __syncthreads();
+  const u64 wlo = wlo_s, whi = whi_s, wn = whi - wlo;
+  const bool in_smem = wn <= (u64)CAP;
+  if (in_smem)
+    for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = B[wlo + i];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 i = a0 + (u64)k * kJoinThreads + threadIdx.x;
+    if (i >= a1) break;
+    const K x = A[i];
+    u64 l, h;
+    if (in_smem) {
+      l = lower_bound_g<K>(win, 0, wn, x);
+      h = upper_bound_g<K>(win, l, wn, x);
+    } else {
+      l = lower_bound_g<K>(B + wlo, 0, wn, x);
+      h = upper_bound_g<K>(B + wlo, l, wn, x);
+    }
+    u32 c = (u32)(h - l);
+    if (nan_key && x == nan_packed) c = 0;
+    lo_out[i] = (u32)(wlo + l);
+    cnt_out[i] = c;
+  }
+}
+
+struct JoinKeyOut {
+  void* keys_out;    // merged key column (dtype of the A side key), or null
+  int dtype;
+  u32 flags;
+  u64 tmin;
+  const void* orig;  // original A key column (float keys are gathered from it)
+};
+
+template <typename K>
+__device__ __forceinline__ void write_join_key(const JoinKeyOut& ko, u64 o, K packed, u32 row) {
+  if (!ko.keys_out) return;
+  if (dtype_is_float(ko.dtype)) store_raw(ko.keys_out, ko.dtype, o, load_raw(ko.orig, ko.dtype, row));
+  else store_raw(ko.keys_out, ko.dtype, o, untransform_int(ko.dtype, ko.flags, (u64)packed + ko.tmin));
+}
+
+// Inner join: output o belongs to the sorted A row i with off[i] <= o < off[i+1].
+template <typename K>
+__global__ void __launch_bounds__(kJoinThreads) k_join_expand_inner(const u64* off, u64 na, u64 m,
+                                                                   const u32* lo, const u32* pA,
+                                                                   const u32* pB, const K* skA,
+                                                                   int32_t* a_out, int32_t* b_out,
+                                                                   JoinKeyOut ko) {
+  constexpr int CAP = 4096;
+  __shared__ u64 win[CAP];
+  __shared__ u64 i0_s, i1_s;
+  const u64 o0 = (u64)blockIdx.x * kJoinTile;
+  const u64 o1 = min(m, o0 + kJoinTile);
+  if (threadIdx.x == 0) {
+    i0_s = upper_bound_g<u64>(off, 0, na, o0) - 1;
+    i1_s = upper_bound_g<u64>(off, i0_s, na, o1 - 1);  // one past the last row used
+  }
+  __syncthreads();
+  const u64 i0 = i0_s, i1 = i1_s, wn = i1 - i0;
+  const bool in_smem = wn <= (u64)CAP;
+  if (in_smem)
+    for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = off[i0 + i];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 o = o0 + (u64)k * kJoinThreads + threadIdx.x;
+    if (o >= o1) break;
+    u64 r;
+    if (in_smem) r = upper_bound_g<u64>(win, 0, wn, o) - 1;
+    else r = upper_bound_g<u64>(off + i0, 0, wn, o) - 1;
+    const u64 i = i0 + r;
+    const u64 base = in_smem ? win[r] : off[i];
+    const u64 j = (u64)lo[i] + (o - base);
+    const u32 ra = pA[i];
+    a_out[o] = (int32_t)ra;
+    b_out[o] = (int32_t)pB[j];
+    write_join_key<K>(ko, o, skA[i], ra);
+  }
+}
+
+// left / right join: one output per sorted A row, first match in B or -1.
+template <typename K>
+__global__ void __launch_bounds__(256) k_join_expand_first(u64 na, const u32* lo, const u32* cnt,
+                                                          const u32* pA, const u32* pB, const K* skA,
+                                                          int32_t* a_out, int32_t* b_out, JoinKeyOut ko) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (u64)gridDim.x * blockDim.x) {
+    const u32 ra = pA[i];
+    a_out[i] = (int32_t)ra;
+    b_out[i] = cnt[i] ? (int32_t)pB[lo[i]] : -1;
+    write_join_key<K>(ko, i, skA[i], ra);
+  }
+}
+
+// ------------------------------------------------------------------ gather ---
+// out[i] = src[idx[i]] converted to out_dtype; idx < 0 -> NaN (float out) or -1.
+__global__ void __launch_bounds__(256) k_gather(const void* src, int sdt, u64 n_src, const int32_t* idx, u64 n,
+                                               void* out, int odt) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const int32_t r = idx[i];
+    if (r < 0 || (u64)r >= n_src) {
+      if (odt == JFX_F32) ((float*)out)[i] = __int_as_float(0x7fc00000);
+      else if (odt == JFX_F64) ((double*)out)[i] = __longlong_as_double(0x7ff8000000000000ll);
+      else store_raw(out, odt, i, ~0ull);
+      continue;
+    }
+    if (odt == sdt) {
+      store_raw(out, odt, i, load_raw(src, sdt, r));
+      continue;
+    }
+    // conversion (integer/bool payload promoted to a float)
+    double x;
+    switch (sdt) {
+      case JFX_F32: x = ((const float*)src)[r]; break;
+      case JFX_F64: x = ((const double*)src)[r]; break;
+      case JFX_I8: x = ((const signed char*)src)[r]; break;
+      case JFX_I16: x = ((const short*)src)[r]; break;
+      case JFX_I32: x = ((const int*)src)[r]; break;
+      case JFX_I64: x = (double)((const long long*)src)[r]; break;
+      case JFX_U8: case JFX_BOOL: x = ((const unsigned char*)src)[r]; break;
+      case JFX_U16: x = ((const unsigned short*)src)[r]; break;
+      case JFX_U32: x = ((const unsigned*)src)[r]; break;
+      default: x = (double)((const unsigned long long*)src)[r]; break;
+    }
+    if (odt == JFX_F32) {
+      // round the integer straight to float32 (double rounding can differ)
+      float f;
+      switch (sdt) {
+        case JFX_I64: f = (float)((const long long*)src)[r]; break;
+        case JFX_U64: f = (float)((const unsigned long long*)src)[r]; break;
+        case JFX_I32: f = (float)((const int*)src)[r]; break;
+        case JFX_U32: f = (float)((const unsigned*)src)[r]; break;
+        default: f = (float)x; break;
+      }
+      ((float*)out)[i] = f;
+    } else if (odt == JFX_F64) {
+      ((double*)out)[i] = x;
+    } else {
+      store_raw(out, odt, i, (u64)(long long)x);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_hash(PackDesc pd, u64 n, u32* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    out[i] = hash_row(pd, i);
+}
+
+__global__ void k_offsets_from_base(const u32* base, int p, u64 n, int64_t* out) {
+  for (int i = threadIdx.x; i <= p; i += blockDim.x) out[i] = i < p ? (int64_t)base[i] : (int64_t)n;
+}
+
+}  // namespace jfx

@@ -1,0 +1,722 @@
+// radix.cuh -- onesweep stable LSD radix sort for sm_100a.
+//
+// Replaces the reference's per-digit XLA comparison sorts
+// (ParallelRadixSort._compute_local_histogram / _compute_global_offsets /
+// _redistribute_data, parallel_algorithms.py:319-424, driven by lax.scan at
+// :508-549) with:
+//   1. one upsweep that reads the key columns once and builds the digit
+//      histograms of every pass (k_hist),
+//   2. an exclusive scan of each histogram (k_hist_scan),
+//   3. one chained-scan kernel per pass (k_onesweep): a CTA takes the next
+//      tile id from an atomic counter, ranks its keys with warp match-any
+//      ballots (stable), publishes its per-digit counts, resolves its global
+//      offsets by decoupled look-back over the preceding tiles (every wait is
+//      bounded and reports DERR_TIMEOUT), sorts the tile by digit in shared
+//      memory and writes each digit run contiguously.
+// Keys are the columns packed into one unsigned word (bit-packing each
+// column's (value - min) after an order-preserving transform), so a
+// multi-column lexicographic sort is one radix sort over ceil(bits / 11)
+// passes whenever the packed width fits 64 bits.
+#pragma once
+
+#include "common.cuh"
+
+namespace jfx {
+
+// look-back status word: [31:30] flag, [29:0] count
+constexpr u32 ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_ERR = 3u << 30, ST_CNT = (1u << 30) - 1;
+
+template <int RB>
+struct RadixCfg {
+  static constexpr int THREADS = RB >= 11 ? 512 : 256;
+  static constexpr int IPT = 16;
+};
+
+template <typename K, int RB>
+struct PassLayout {
+  static constexpr int THREADS = RadixCfg<RB>::THREADS, IPT = RadixCfg<RB>::IPT;
+  static constexpr int RADIX = 1 << RB, WARPS = THREADS / 32, TILE = THREADS * IPT;
+  static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 2;
+  static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
+  static constexpr size_t A_BYTES = HIST_BYTES > KEY_BYTES ? HIST_BYTES : KEY_BYTES;
+  static constexpr size_t VAL_BYTES = (size_t)TILE * 4;
+  static constexpr size_t SMEM = A_BYTES + VAL_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
+};
+
+// Digit / key modes of one pass.
+enum : int {
+  KEY_PACK = 0,   // first pass packs the key columns (pack_row)
+  KEY_HASH = 1,   // first pass hashes the key columns (hash_multi_columns)
+  DIG_BITS = 0,   // digit = (key >> shift) & mask
+  DIG_MOD = 1,    // digit = key % modulus (hash partition)
+};
+
+struct PassArgs {
+  const void* keys_in;   // K[n] (not read by the first pass)
+  const u32* vals_in;    // u32[n] (not read by the first pass)
+  void* keys_out;        // K[n]
+  u32* vals_out;         // u32[n]
+  const u32* bin_base;   // [RADIX] exclusive global digit offsets of this pass
+  u32* status;           // [tiles][RADIX] look-back words of this pass (zeroed)
+  u32* status_next;      // [tiles][RADIX] to clear for the following pass, or null
+  u32* tile_counter;     // zeroed counter for tile ids of this pass
+  u32* err;              // device error word
+  const u32* gather_idx; // first pass: rows are read through this index, or null
+  u64 n;
+  int shift, width;
+  int key_mode, digit_mode;
+  u32 modulus;
+  int reverse;           // write position n-1-p (descending radix sort)
+  PackDesc pack;
+};
+
+__device__ __forceinline__ u32 fmix32(u32 h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Key column as the hash reads it (parallel_algorithms.py:89-93, 113-121).
+__device__ __forceinline__ u32 hash_word(const ColDesc& c, size_t row, bool multi) {
+  switch (c.dtype) {
+    case JFX_F32: return __ldg((const u32*)c.ptr + row);
+    case JFX_F64: {
+      double x = __ldg((const double*)c.ptr + row);
+      float f = (float)x;
+      return __float_as_uint(f);
+    }
+    case JFX_I64: case JFX_U64: return (u32)__ldg((const u64*)c.ptr + row);
+    case JFX_I32: case JFX_U32: return __ldg((const u32*)c.ptr + row);
+    case JFX_I16: return (u32)(int)((const short*)c.ptr)[row];
+    case JFX_I8: return (u32)(int)((const signed char*)c.ptr)[row];
+    case JFX_U16: return ((const unsigned short*)c.ptr)[row];
+    case JFX_U8: case JFX_BOOL: return ((const unsigned char*)c.ptr)[row];
+  }
+  return 0;
+}
+
+// hash_multi_columns (parallel_algorithms.py:69-136).
+__device__ __forceinline__ u32 hash_row(const PackDesc& pd, size_t row) {
+  if (pd.ncols == 1) return fmix32(hash_word(pd.c[0], row, false));
+  u32 h = 0x1337u;
+  for (int i = 0; i < pd.ncols; ++i) {
+    u32 k = hash_word(pd.c[i], row, true);
+    h ^= k * (0x9e3779b1u + (u32)i);
+    h = (h << 13) | (h >> 19);
+    h *= 0x85ebca6bu;
+  }
+  return fmix32(h);
+}
+
+template <typename K>
+__device__ __forceinline__ u32 digit_of(K key, int mode, int shift, u32 mask, u32 modulus) {
+  if (mode == DIG_MOD) return (u32)key % modulus;
+  return (u32)(key >> shift) & mask;
+}
+
+// Exclusive scan of data[0..N) in shared memory by all THREADS threads.
+template <int THREADS, int N>
+__device__ __forceinline__ void block_exclusive_scan(u32* data, u32* scratch) {
+  constexpr int PER = N >= THREADS ? N / THREADS : 1;
+  constexpr int ACTIVE = N >= THREADS ? THREADS : N;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  u32 local[PER];
+  u32 sum = 0;
+  if (tid < ACTIVE) {
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      local[k] = data[tid * PER + k];
+      sum += local[k];
+    }
+  }
+  u32 x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    u32 y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) scratch[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    u32 w = lane < THREADS / 32 ? scratch[lane] : 0u;
+    u32 inc = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      u32 y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    scratch[lane] = inc - w;
+  }
+  __syncthreads();
+  u32 ex = x - sum + scratch[warp];
+  if (tid < ACTIVE) {
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      data[tid * PER + k] = ex;
+      ex += local[k];
+    }
+  }
+  __syncthreads();
+}
+
+// Bounded spin on a look-back word until its flag is set.  Returns the word, or
+// ST_ERR after kSpinLimitNs or when another CTA already reported a timeout.
+__device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
+  u32 v = ld_relaxed(p);
+  if (v & 0xC0000000u) return v;
+  u64 t0 = globaltimer_ns();
+  for (u32 spins = 1;; ++spins) {
+    v = ld_relaxed(p);
+    if (v & 0xC0000000u) return v;
+    if (spins > 128) __nanosleep(64);
+    if ((spins & 255u) == 0) {
+      if (ld_relaxed(err) & DERR_TIMEOUT) return ST_ERR;
+      if (globaltimer_ns() - t0 > kSpinLimitNs) {
+        atomicOr(err, DERR_TIMEOUT);
+        return ST_ERR;
+      }
+    }
+  }
+}
+
+template <typename K, int RB, bool FIRST>
+__global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
+  using L = PassLayout<K, RB>;
+  constexpr int THREADS = L::THREADS, IPT = L::IPT, RADIX = L::RADIX, WARPS = L::WARPS,
+                TILE = L::TILE;
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint16_t* whist = (uint16_t*)smem;  // [WARPS][RADIX] during ranking
+  K* skeys = (K*)smem;                // [TILE] after ranking (aliases whist)
+  u32* svals = (u32*)(smem + L::A_BYTES);
+  u32* sexcl = svals + TILE;  // tile digit counts, then the tile's exclusive prefix
+  u32* sbase = sexcl + RADIX; // global position of the tile's first key of each digit
+  u32* sscan = sbase + RADIX; // 32 words of block-scan scratch
+  u32* sflag = sscan + 32;    // [0] tile id, [1] abort
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    sflag[0] = atomicAdd(a.tile_counter, 1u);
+    sflag[1] = 0;
+  }
+  for (int i = tid; i < WARPS * RADIX / 2; i += THREADS) ((u32*)whist)[i] = 0u;
+  __syncthreads();
+  const u32 tile = sflag[0];
+  const u64 base = (u64)tile * TILE;
+  const u32 tile_n = (u32)min((u64)TILE, a.n - base);
+  const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
+
+  K key[IPT];
+  u32 val[IPT], dig[IPT];
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 off = warp * 32 * IPT + i * 32 + lane;
+    dig[i] = RADIX;
+    if (off < tile_n) {
+      const u64 idx = base + off;
+      if (FIRST) {
+        const u64 row = a.gather_idx ? (u64)a.gather_idx[idx] : idx;
+        key[i] = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, row) : pack_row<K>(a.pack, row);
+        val[i] = (u32)row;
+      } else {
+        key[i] = ((const K*)a.keys_in)[idx];
+        val[i] = a.vals_in[idx];
+      }
+      dig[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus);
+    }
+  }
+
+  // Stable rank within the warp: lanes holding the same digit are ranked by
+  // lane, and items are visited in row order, so equal digits keep row order.
+  u32 rank[IPT];
+  const u32 lt = lanemask_lt(), gt = lanemask_gt();
+  uint16_t* wh = whist + warp * RADIX;
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 d = dig[i];
+    const u32 peers = __match_any_sync(0xffffffffu, d);
+    const bool valid = d < (u32)RADIX;
+    const u32 prior = valid ? (u32)wh[d] : 0u;
+    rank[i] = prior + __popc(peers & lt);
+    __syncwarp();
+    if (valid && !(peers & gt)) wh[d] = (uint16_t)(prior + __popc(peers));
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: exclusive prefix over warps (in place) and the tile count.
+  for (int d = tid; d < RADIX; d += THREADS) {
+    u32 run = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const u32 c = whist[w * RADIX + d];
+      whist[w * RADIX + d] = (uint16_t)run;
+      run += c;
+    }
+    sexcl[d] = run;
+  }
+  __syncthreads();
+
+  // Publish this tile's counts, then resolve the prefix over earlier tiles.
+  u32* st = a.status + (u64)tile * RADIX;
+  for (int d = tid; d < RADIX; d += THREADS)
+    st_relaxed(st + d, (tile == 0 ? ST_INC : ST_AGG) | sexcl[d]);
+  for (int d = tid; d < RADIX; d += THREADS) {
+    u32 excl = 0;
+    bool bad = false;
+    if (tile > 0) {
+      const u32* p = a.status + (u64)(tile - 1) * RADIX + d;
+      for (u32 k = tile;; --k) {
+        const u32 v = wait_status(p, a.err);
+        const u32 f = v & 0xC0000000u;
+        if (f == ST_ERR) { bad = true; break; }
+        excl += v & ST_CNT;
+        if (f == ST_INC || k == 1) break;
+        p -= RADIX;
+      }
+      st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + sexcl[d])));
+    }
+    if (bad) sflag[1] = 1u;
+    sbase[d] = a.bin_base[d] + excl;
+  }
+  __syncthreads();
+  if (sflag[1]) return;
+
+  block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);
+
+  u32 pos[IPT];
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 d = dig[i];
+    pos[i] = d < (u32)RADIX ? sexcl[d] + (u32)whist[warp * RADIX + d] + rank[i] : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    if (dig[i] < (u32)RADIX) {
+      skeys[pos[i]] = key[i];
+      svals[pos[i]] = val[i];
+    }
+  }
+  __syncthreads();
+
+  K* kout = (K*)a.keys_out;
+  for (u32 j = tid; j < tile_n; j += THREADS) {
+    const K k = skeys[j];
+    const u32 d = digit_of<K>(k, a.digit_mode, a.shift, mask, a.modulus);
+    u64 g = (u64)sbase[d] + (j - sexcl[d]);
+    if (g >= a.n) {  // only reachable if histogram and pass disagree
+      atomicOr(a.err, DERR_BOUNDS);
+      continue;
+    }
+    if (a.reverse) g = a.n - 1 - g;
+    kout[g] = k;
+    a.vals_out[g] = svals[j];
+  }
+  if (a.status_next)
+    for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
+}
+
+// ----------------------------------------------------------------- upsweep ---
+struct HistArgs {
+  PackDesc pack;
+  u32* hist;       // [npass][RADIX], zeroed
+  u32* targets;    // optional: digit of pass 0 per row (hash partition targets)
+  u64 n;
+  int npass;
+  int key_mode, digit_mode;
+  u32 modulus;
+  int shift[8];
+  int width[8];
+};
+
+template <typename K, int RB>
+__global__ void __launch_bounds__(256) k_hist(HistArgs a) {
+  constexpr int RADIX = 1 << RB;
+  extern __shared__ u32 sh[];
+  const int total = a.npass * RADIX;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) sh[i] = 0u;
+  __syncthreads();
+  u32 mask[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) mask[p] = a.width[p] >= 32 ? 0xffffffffu : ((1u << a.width[p]) - 1u);
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < a.n; r += stride) {
+    const K k = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, r) : pack_row<K>(a.pack, r);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      if (p >= a.npass) break;
+      const u32 d = digit_of<K>(k, a.digit_mode, a.shift[p], mask[p], a.modulus);
+      atomicAdd(&sh[p * RADIX + d], 1u);
+      if (p == 0 && a.targets) a.targets[r] = d;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < total; i += blockDim.x)
+    if (sh[i]) atomicAdd(&a.hist[i], sh[i]);
+}
+
+// Exclusive scan of each pass's histogram (one CTA per pass).
+template <int RB>
+__global__ void __launch_bounds__(1024) k_hist_scan(const u32* hist, u32* base) {
+  constexpr int RADIX = 1 << RB;
+  __shared__ u32 data[RADIX];
+  __shared__ u32 scratch[32];
+  const u32* h = hist + (u64)blockIdx.x * RADIX;
+  for (int i = threadIdx.x; i < RADIX; i += 1024) data[i] = h[i];
+  __syncthreads();
+  block_exclusive_scan<1024, RADIX>(data, scratch);
+  for (int i = threadIdx.x; i < RADIX; i += 1024) base[(u64)blockIdx.x * RADIX + i] = data[i];
+}
+
+// ---------------------------------------------------------------- min/max ---
+// Min and max of every column's transformed value.  out[2j] = min, out[2j+1] = max.
+__global__ void __launch_bounds__(256) k_minmax(PackDesc pd, u64 n, u64* out) {
+  u64 mn[kMaxCols], mx[kMaxCols];
+#pragma unroll
+  for (int j = 0; j < kMaxCols; ++j) {
+    mn[j] = ~0ull;
+    mx[j] = 0ull;
+  }
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+#pragma unroll
+    for (int j = 0; j < kMaxCols; ++j) {
+      if (j >= pd.ncols) break;
+      const u64 t = load_t(pd.c[j], r);
+      mn[j] = t < mn[j] ? t : mn[j];
+      mx[j] = t > mx[j] ? t : mx[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kMaxCols; ++j) {
+    if (j >= pd.ncols) break;
+    u64 a = mn[j], b = mx[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const u64 a2 = __shfl_xor_sync(0xffffffffu, a, o);
+      const u64 b2 = __shfl_xor_sync(0xffffffffu, b, o);
+      a = a2 < a ? a2 : a;
+      b = b2 > b ? b2 : b;
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&out[2 * j], a);
+      atomicMax(&out[2 * j + 1], b);
+    }
+  }
+}
+
+__global__ void k_init_minmax(u64* out, int ncols) {
+  int j = threadIdx.x;
+  if (j < ncols) {
+    out[2 * j] = ~0ull;
+    out[2 * j + 1] = 0ull;
+  }
+}
+
+__global__ void k_iota(u32* out, u64 n, int reverse) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    out[i] = reverse ? (u32)(n - 1 - i) : (u32)i;
+}
+
+template <typename K>
+__global__ void k_fill_keys(K* out, u64 n) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    out[i] = (K)0;
+}
+
+// ----------------------------------------------------------- host driver ---
+// Pinned host scratch for the few words an entry point reads back.
+struct HostScratch {
+  u64* p = nullptr;
+  ~HostScratch() {
+    if (p) cudaFreeHost(p);
+  }
+  u64* get() {
+    if (!p && cudaMallocHost((void**)&p, 4096) != cudaSuccess) p = nullptr;
+    return p;
+  }
+};
+extern thread_local HostScratch g_host;
+
+// Column ranges -> packing (shift/bits per column, most significant first).
+struct KeyPlan {
+  PackDesc pack;
+  int total_bits = 0;
+  u64 tmax[kMaxCols];
+};
+
+// Fill `cols` from jfx_column descriptors (validates dtypes).
+inline int build_pack(const jfx_column* in, int ncols, u32 extra_flags, bool allow_desc, PackDesc& pd) {
+  if (ncols < 1 || ncols > kMaxCols) return fail(JFX_ERR_ARG, "1..%d key columns supported, got %d", kMaxCols, ncols);
+  memset(&pd, 0, sizeof pd);
+  pd.ncols = ncols;
+  for (int j = 0; j < ncols; ++j) {
+    if (!in[j].data) return fail(JFX_ERR_ARG, "key column %d has a null pointer", j);
+    if (dtype_size(in[j].dtype) == 0) return fail(JFX_ERR_DTYPE, "key column %d: unsupported dtype %d", j, in[j].dtype);
+    pd.c[j].ptr = in[j].data;
+    pd.c[j].dtype = in[j].dtype;
+    pd.c[j].flags = extra_flags | ((allow_desc && (in[j].flags & JFX_COL_DESC)) ? CF_DESC : 0u);
+    if ((pd.c[j].flags & CF_DESC) && in[j].dtype == JFX_BOOL)
+      return fail(JFX_ERR_DTYPE, "descending bool key (max(x) - x) is not defined for bool");
+    if (dtype_is_float(in[j].dtype)) pd.nan_cols |= 1 << j;
+  }
+  return JFX_OK;
+}
+
+inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s) {
+  k_init_minmax<<<1, 32, 0, s>>>(dev_out, pd.ncols), note_launch();
+  if (n) {
+    int grid = (int)std::min<u64>((n + 255) / 256, (u64)device_sm_count() * 8);
+    k_minmax<<<grid, 256, 0, s>>>(pd, n, dev_out), note_launch();
+  }
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+// Computes min/max of every key column (two reductions when an integer column
+// is descending: max(x) first, then the rewritten values) and assigns the bit
+// fields.  One stream synchronisation.
+inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s) {
+  PackDesc& pd = kp.pack;
+  u64* host = g_host.get();
+  if (!host) return fail(JFX_ERR_CUDA, "cudaMallocHost failed");
+  bool need_raw_max = false;
+  for (int j = 0; j < pd.ncols; ++j)
+    if ((pd.c[j].flags & CF_DESC) && !dtype_is_float(pd.c[j].dtype)) need_raw_max = true;
+  if (need_raw_max && n) {
+    PackDesc raw = pd;
+    for (int j = 0; j < raw.ncols; ++j) raw.c[j].flags &= ~(CF_DESC | CF_QUIRK);
+    JFX_TRY(launch_minmax(raw, n, dev_scratch, s));
+    JFX_CUDA(cudaMemcpyAsync(host, dev_scratch, 2 * pd.ncols * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    JFX_CUDA(cudaStreamSynchronize(s));
+    for (int j = 0; j < pd.ncols; ++j)
+      if ((pd.c[j].flags & CF_DESC) && !dtype_is_float(pd.c[j].dtype)) {
+        u64 raw_max = untransform_int(pd.c[j].dtype, 0, host[2 * j + 1]);
+        // sign-extend narrow signed types so (short)desc_max is the max value
+        pd.c[j].desc_max = raw_max;
+      }
+  }
+  JFX_TRY(launch_minmax(pd, n, dev_scratch, s));
+  JFX_CUDA(cudaMemcpyAsync(host, dev_scratch, 2 * pd.ncols * sizeof(u64), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  int shift = 0;
+  kp.total_bits = 0;
+  for (int j = pd.ncols - 1; j >= 0; --j) {
+    ColDesc& c = pd.c[j];
+    u64 mn = host[2 * j], mx = host[2 * j + 1];
+    if (n == 0) mn = mx = 0;
+    c.tmin = mn;
+    kp.tmax[j] = mx;
+    c.bits = bit_length(mx - mn);
+    c.shift = shift;
+    shift += c.bits;
+  }
+  kp.total_bits = shift;
+  return JFX_OK;
+}
+
+// Workspace of one radix sort of n rows (worst case: 64-bit keys).
+struct SortBuffers {
+  void* keys[2];   // ping-pong packed keys
+  u32* vals[2];    // ping-pong row ids
+  u32* hist;       // [8][2048]
+  u32* base;       // [8][2048]
+  u32* counters;   // [8]
+  u32* status[2];  // [tiles][RADIX] ping-pong look-back words
+  u64 status_words;
+};
+
+inline u64 max_status_words(u64 n) {
+  // the largest tiles x RADIX over the kernel configurations used
+  u64 w8 = (u64)ceil_div(n ? n : 1, PassLayout<u64, 8>::TILE) * 256;
+  u64 w9 = (u64)ceil_div(n ? n : 1, PassLayout<u64, 9>::TILE) * 512;
+  u64 w10 = (u64)ceil_div(n ? n : 1, PassLayout<u64, 10>::TILE) * 1024;
+  u64 w11 = (u64)ceil_div(n ? n : 1, PassLayout<u64, 11>::TILE) * 2048;
+  return std::max(std::max(w8, w9), std::max(w10, w11));
+}
+
+inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b) {
+  b.keys[0] = ar.take<u64>(n ? n : 1);
+  b.keys[1] = ar.take<u64>(n ? n : 1);
+  b.vals[0] = ar.take<u32>(n ? n : 1);
+  b.vals[1] = ar.take<u32>(n ? n : 1);
+  b.hist = ar.take<u32>(8 * 2048);
+  b.base = ar.take<u32>(8 * 2048);
+  b.counters = ar.take<u32>(64);
+  b.status_words = max_status_words(n);
+  b.status[0] = ar.take<u32>(b.status_words);
+  b.status[1] = ar.take<u32>(b.status_words);
+}
+
+template <typename K, int RB, bool FIRST>
+inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s) {
+  using L = PassLayout<K, RB>;
+  static bool attr_set = false;  // per instantiation
+  if (!attr_set) {
+    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)L::SMEM));
+    attr_set = true;
+  }
+  int tiles = ceil_div(n, L::TILE);
+  const long t = timing_begin(s);
+  k_onesweep<K, RB, FIRST><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
+  if (t >= 0) {
+    // algorithmic bytes: the first pass reads the key columns and writes
+    // key + row id; later passes read and write key + row id
+    double kraw = 0;
+    if (FIRST) {
+      for (int j = 0; j < a.pack.ncols; ++j) kraw += dtype_size(a.pack.c[j].dtype);
+      if (a.gather_idx) kraw += 4;
+    }
+    const double per = FIRST ? kraw + sizeof(K) + 4 : 2.0 * (sizeof(K) + 4);
+    timing_end(t, s, per * (double)n);
+  }
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+struct RadixRequest {
+  PackDesc pack;
+  int key_mode = KEY_PACK;
+  int digit_mode = DIG_BITS;
+  u32 modulus = 0;
+  int total_bits = 0;        // packed key width (DIG_BITS)
+  int max_digit_bits = 11;   // widest digit allowed
+  bool reverse = false;      // descending: write n-1-p in the last pass
+  const u32* gather_idx = nullptr;
+  u32* targets = nullptr;    // hash partition: digit of each row (row order)
+  u32* perm_out = nullptr;   // sorted row ids
+  void* keys_out = nullptr;  // sorted packed keys (K), may be null -> internal buffer
+  bool key64 = false;        // packed key type
+  void* keys_result = nullptr; // filled: where the sorted packed keys ended up
+  int npass = 0;               // filled: passes run
+};
+
+template <typename K, int RB>
+inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
+  constexpr int RADIX = 1 << RB;
+  int npass;
+  int shift[8] = {0}, width[8] = {0};
+  if (rq.digit_mode == DIG_MOD) {
+    npass = 1;
+    width[0] = RB;
+  } else {
+    npass = ceil_div(rq.total_bits, rq.max_digit_bits);
+    if (npass > 8) return fail(JFX_ERR_ARG, "too many radix passes");
+    int base_w = rq.total_bits / npass, rem = rq.total_bits % npass, at = 0;
+    for (int p = 0; p < npass; ++p) {
+      width[p] = base_w + (p < rem ? 1 : 0);
+      shift[p] = at;
+      at += width[p];
+    }
+  }
+  rq.npass = npass;
+  JFX_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)npass * RADIX * sizeof(u32), s));
+  JFX_CUDA(cudaMemsetAsync(b.counters, 0, 64 * sizeof(u32), s));
+  const u64 tiles = (u64)ceil_div(n, PassLayout<K, RB>::TILE);
+  JFX_CUDA(cudaMemsetAsync(b.status[0], 0, tiles * RADIX * sizeof(u32), s));
+
+  HistArgs h;
+  memset(&h, 0, sizeof h);
+  h.pack = rq.pack;
+  h.hist = b.hist;
+  h.targets = rq.targets;
+  h.n = n;
+  h.npass = npass;
+  h.key_mode = rq.key_mode;
+  h.digit_mode = rq.digit_mode;
+  h.modulus = rq.modulus;
+  for (int p = 0; p < 8; ++p) {
+    h.shift[p] = shift[p];
+    h.width[p] = width[p];
+  }
+  {
+    int grid = (int)std::min<u64>((n + 1023) / 1024, (u64)device_sm_count() * 4);
+    size_t smem = (size_t)npass * RADIX * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+      JFX_CUDA(cudaFuncSetAttribute(k_hist<K, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
+      attr = true;
+    }
+    k_hist<K, RB><<<std::max(grid, 1), 256, smem, s>>>(h), note_launch();
+    JFX_CUDA(cudaGetLastError());
+  }
+  k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
+  JFX_CUDA(cudaGetLastError());
+
+  u32* out_vals = rq.perm_out;
+  void* out_keys = rq.keys_out ? rq.keys_out : b.keys[(npass - 1) & 1];
+  for (int p = 0; p < npass; ++p) {
+    PassArgs a;
+    memset(&a, 0, sizeof a);
+    const bool last = p == npass - 1;
+    a.keys_in = p ? b.keys[(p - 1) & 1] : nullptr;
+    a.vals_in = p ? b.vals[(p - 1) & 1] : nullptr;
+    a.keys_out = last ? out_keys : b.keys[p & 1];
+    a.vals_out = last ? out_vals : b.vals[p & 1];
+    a.bin_base = b.base + (u64)p * RADIX;
+    a.status = b.status[p & 1];
+    a.status_next = last ? nullptr : b.status[(p + 1) & 1];
+    a.tile_counter = b.counters + p;
+    a.err = err;
+    a.gather_idx = rq.gather_idx;
+    a.n = n;
+    a.shift = shift[p];
+    a.width = width[p];
+    a.key_mode = rq.key_mode;
+    a.digit_mode = rq.digit_mode;
+    a.modulus = rq.modulus;
+    a.reverse = last && rq.reverse;
+    a.pack = rq.pack;
+    if (p == 0) {
+      JFX_TRY((launch_pass<K, RB, true>(a, n, s)));
+    } else {
+      JFX_TRY((launch_pass<K, RB, false>(a, n, s)));
+    }
+  }
+  rq.keys_result = out_keys;
+  return JFX_OK;
+}
+
+template <typename K>
+inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
+  int rb;
+  if (rq.digit_mode == DIG_MOD) {
+    rb = rq.modulus <= 256 ? 8 : rq.modulus <= 512 ? 9 : rq.modulus <= 1024 ? 10 : 11;
+  } else {
+    int npass = ceil_div(rq.total_bits, rq.max_digit_bits);
+    int w = ceil_div(rq.total_bits, npass);
+    rb = w <= 8 ? 8 : w;
+  }
+  switch (rb) {
+    case 8: return run_radix<K, 8>(rq, n, b, err, s);
+    case 9: return run_radix<K, 9>(rq, n, b, err, s);
+    case 10: return run_radix<K, 10>(rq, n, b, err, s);
+    case 11: return run_radix<K, 11>(rq, n, b, err, s);
+  }
+  return fail(JFX_ERR_ARG, "digit width %d unsupported", rb);
+}
+
+// Sorts rows by the packed key (or hash digit).  n >= 1.  With total_bits == 0
+// (every key equal) the stable order is the identity.
+inline int radix_sort(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
+  if (n > (u64)kMaxRows) return fail(JFX_ERR_CAPACITY, "%llu rows exceed the %lld-row limit", n, (long long)kMaxRows);
+  if (rq.digit_mode == DIG_BITS && rq.total_bits == 0) {
+    int grid = (int)std::min<u64>((n + 255) / 256, 4096);
+    k_iota<<<std::max(grid, 1), 256, 0, s>>>(rq.perm_out, n, rq.reverse ? 1 : 0), note_launch();
+    void* out_keys = rq.keys_out ? rq.keys_out : b.keys[0];
+    if (rq.key64) k_fill_keys<u64><<<std::max(grid, 1), 256, 0, s>>>((u64*)out_keys, n), note_launch();
+    else k_fill_keys<u32><<<std::max(grid, 1), 256, 0, s>>>((u32*)out_keys, n), note_launch();
+    JFX_CUDA(cudaGetLastError());
+    rq.keys_result = out_keys;
+    rq.npass = 0;
+    return JFX_OK;
+  }
+  if (rq.key64) return run_radix_k<u64>(rq, n, b, err, s);
+  return run_radix_k<u32>(rq, n, b, err, s);
+}
+
+}  // namespace jfx

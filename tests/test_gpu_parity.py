@@ -1,0 +1,326 @@
+"""GPU parity: the product API (through libjfx.so) against the oracle and the
+reference tests' known answers.  Bit-exact for orders, keys, counts, min/max,
+index pairs and partition assignments; float sums within 2^-16 * sum(|x|)
+per group (the tolerance of the north-star contract)."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import jfx_oracle as O
+from _kat import check_kat, load_kats
+
+pytestmark = pytest.mark.gpu
+
+KATS = load_kats()
+
+
+def _np(t):
+    if isinstance(t, torch.Tensor):
+        t = t.cpu()
+        if t.dtype in (torch.uint16, torch.uint32, torch.uint64):
+            return t.numpy()
+        return t.numpy()
+    return np.asarray(t)
+
+
+@pytest.fixture(scope="module")
+def P():
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from jaxframes_b200 import build
+    build.build()
+    import jaxframes_b200.parallel_algorithms as P
+    return P
+
+
+class ProductImpl:
+    def __init__(self, P):
+        self.P = P
+
+    def parallel_sort(self, keys, values, ascending):
+        if values is None:
+            return _np(self.P.parallel_sort(keys, ascending=ascending)), None
+        sk, sv = self.P.parallel_sort(keys, values=values, ascending=ascending)
+        return _np(sk), _np(sv)
+
+    def lexsort(self, keys, ascending):
+        return _np(self.P.multi_column_lexsort(keys, ascending))
+
+    def groupby(self, keys, values, aggs):
+        uk, out = self.P.groupby_aggregate(keys, values, aggs)
+        return _np(uk), {c: _np(v) for c, v in out.items()}
+
+    def groupby_multi(self, keys, names, values, aggs):
+        uk, out = self.P.groupby_aggregate_multi_column(keys, names, values, aggs)
+        return {n: _np(v) for n, v in uk.items()}, {c: _np(v) for c, v in out.items()}
+
+    def join(self, lk, lv, rk, rv, how):
+        mk, out = self.P.sort_merge_join(lk, lv, rk, rv, how)
+        return _np(mk), {c: _np(v) for c, v in out.items()}
+
+    def join_multi(self, lk, rk, how):
+        j = self.P.ParallelSortMergeJoin()
+        li, ri = j.join_multi_indices(lk, rk, how)
+        return _np(li), _np(ri)
+
+    def hash(self, keys):
+        return _np(self.P.hash_multi_columns(keys))
+
+    def partition(self, keys, p):
+        t, perm, offs = self.P.hash_partition(keys, p)
+        return _np(t), _np(perm), _np(offs)
+
+
+@pytest.mark.parametrize("kat", KATS, ids=[k["name"] for k in KATS])
+def test_product_kat(P, kat):
+    check_kat(kat, ProductImpl(P))
+
+
+# ----------------------------------------------------------------- sorting ---
+SIZES = [1, 2, 31, 32, 33, 255, 4095, 4096, 4097, 8191, 8192, 8193, 100_000, 1_000_003]
+
+
+def _keys(rng, dt, n, kind):
+    info = np.iinfo(dt) if np.issubdtype(dt, np.integer) else None
+    if kind == "full":
+        if info is not None:
+            return rng.integers(info.min, info.max, n, dtype=dt, endpoint=True)
+        x = rng.standard_normal(n).astype(dt) * 1e3
+        x[rng.integers(0, n, max(1, n // 50))] = np.nan
+        x[rng.integers(0, n, max(1, n // 50))] = -0.0
+        x[rng.integers(0, n, max(1, n // 50))] = 0.0
+        x[rng.integers(0, n, max(1, n // 100))] = np.inf
+        return x
+    if kind == "small":
+        return rng.integers(0, 7, n).astype(dt)
+    if kind == "equal":
+        return np.full(n, 5, dtype=dt)
+    if kind == "desc":
+        return np.arange(n, 0, -1).astype(dt)
+    if kind == "heavy":
+        x = rng.integers(0, 1 << 20, n).astype(dt)
+        x[rng.random(n) < 0.6] = 12345
+        return x
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("dt", [np.int32, np.int64, np.uint32, np.uint64, np.float32, np.float64, np.int16])
+@pytest.mark.parametrize("kind", ["full", "small", "equal", "desc", "heavy"])
+def test_radix_sort_matches_oracle(P, dt, kind):
+    rng = np.random.default_rng(hash((np.dtype(dt).name, kind)) & 0xffff)
+    for n in SIZES:
+        k = _keys(rng, dt, n, kind)
+        for asc in (True, False):
+            sk, perm = P.ParallelRadixSort().sort(k, np.arange(n, dtype=np.int32), asc)
+            ek, ep = O.radix_sort(k, np.arange(n), asc)
+            np.testing.assert_array_equal(_np(perm), ep, err_msg=f"n={n} asc={asc}")
+            np.testing.assert_array_equal(_np(sk).view(np.uint8), ek.view(np.uint8), err_msg=f"n={n}")
+
+
+@pytest.mark.parametrize("ncols", [2, 3])
+def test_lexsort_matches_oracle(P, ncols):
+    rng = np.random.default_rng(11 + ncols)
+    for n in [1, 33, 4097, 50_000]:
+        cols = [rng.integers(-5, 5, n).astype(np.int32), rng.standard_normal(n).round(1).astype(np.float32),
+                rng.integers(0, 3, n).astype(np.int64)][:ncols]
+        for asc in [True, [True, False, True][:ncols], [False] * ncols]:
+            got = _np(P.multi_column_lexsort(cols, asc))
+            exp = O.multi_column_lexsort(cols, asc)
+            np.testing.assert_array_equal(got, exp, err_msg=f"n={n} asc={asc}")
+
+
+def test_lexsort_wide_keys_multi_round(P):
+    """Packed width above 64 bits: LSD rounds over column groups."""
+    rng = np.random.default_rng(4)
+    n = 20_000
+    cols = [rng.integers(-2**62, 2**62, n), rng.integers(-2**62, 2**62, n), rng.integers(0, 4, n)]
+    cols[0][::3] = cols[0][1]
+    cols[1][::5] = cols[1][2]
+    got = _np(P.multi_column_lexsort(cols, [True, False, True]))
+    exp = O.multi_column_lexsort(cols, [True, False, True])
+    np.testing.assert_array_equal(got, exp)
+
+
+# ----------------------------------------------------------------- groupby ---
+def _check_group_outputs(got, exp, vals_sorted_abs_sums=None):
+    for c in exp:
+        g, e = got[c], exp[c]
+        assert g.dtype == e.dtype, (c, g.dtype, e.dtype)
+        if np.issubdtype(e.dtype, np.floating):
+            tol = vals_sorted_abs_sums[c] * 2.0 ** -16 if vals_sorted_abs_sums else 0
+            np.testing.assert_allclose(g.astype(np.float64), e.astype(np.float64), rtol=0, atol=0,
+                                       err_msg=c) if tol is 0 else \
+                np.testing.assert_array_less(np.abs(g.astype(np.float64) - e.astype(np.float64)),
+                                             tol + 1e-30, err_msg=c)
+        else:
+            np.testing.assert_array_equal(g, e, err_msg=c)
+
+
+def _abs_sums_single(keys, v):
+    uk, a = O.groupby_aggregate(keys, {"v": np.abs(v.astype(np.float64))}, {"v": "sum"})
+    return a["v"]
+
+
+@pytest.mark.parametrize("n", [1, 5, 512, 513, 8192, 100_000, 1_000_000])
+def test_groupby_single_key(P, n):
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, max(1, n // 7), n).astype(np.int32)
+    v32 = rng.standard_normal(n).astype(np.float32)
+    vi = rng.integers(-1000, 1000, n).astype(np.int32)
+    vals = {"a": v32, "b": vi, "c": v32, "d": v32, "e": vi, "f": vi, "g": v32}
+    aggs = {"a": "sum", "b": "sum", "c": "mean", "d": "max", "e": "min", "f": "count", "g": "count"}
+    uk, out = P.groupby_aggregate(keys, vals, aggs)
+    ek, eout = O.groupby_aggregate(keys, vals, aggs)
+    np.testing.assert_array_equal(_np(uk), ek)
+    got = {c: _np(t) for c, t in out.items()}
+    asum = _abs_sums_single(keys, v32)
+    cnt = np.bincount(np.unique(keys, return_inverse=True)[1])
+    for c in aggs:
+        g, e = got[c], eout[c]
+        assert g.dtype == e.dtype, (c, g.dtype, e.dtype)
+        if c == "a":
+            assert (np.abs(g.astype(np.float64) - e) <= asum * 2.0 ** -16 + 1e-30).all()
+        elif c == "c":
+            assert (np.abs(g.astype(np.float64) - e) <= asum / cnt * 2.0 ** -16 + 1e-30).all()
+        else:
+            np.testing.assert_array_equal(g, e, err_msg=c)
+
+
+def test_groupby_multi_key_c3_like(P):
+    """Shapes of the 100M-row multi-key config, at 2M rows."""
+    rng = np.random.default_rng(42 + 2)
+    n = 2_000_000
+    ranks = np.arange(1, 1_000_001, dtype=np.float64)
+    cdf = np.cumsum(ranks ** -1.1)
+    cdf /= cdf[-1]
+    perm = rng.permutation(1_000_000)
+    k1 = perm[np.searchsorted(cdf, rng.random(n))].astype(np.int32)
+    k2 = rng.integers(0, 64, n).astype(np.int32)
+    v1 = rng.standard_normal(n).astype(np.float32)
+    v2 = rng.integers(-1_000_000, 1_000_001, n).astype(np.int64)
+    vals = {f"v1_{a}": v1 for a in ("sum", "mean", "min", "max", "count")}
+    vals.update({f"v2_{a}": v2 for a in ("sum", "mean", "min", "max", "count")})
+    aggs = {c: c.split("_")[1] for c in vals}
+    uk, out = P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)
+    ek, eout = O.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)
+    np.testing.assert_array_equal(_np(uk["k1"]), ek["k1"])
+    np.testing.assert_array_equal(_np(uk["k2"]), ek["k2"])
+    _, asum = O.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], {"x": np.abs(v1).astype(np.float64)},
+                                               {"x": "sum"})
+    asum = asum["x"]
+    cnt = eout["v1_count"]
+    for c in aggs:
+        g = _np(out[c])
+        e = eout[c]
+        assert g.dtype == e.dtype, (c, g.dtype, e.dtype)
+        if c == "v1_sum":
+            assert (np.abs(g.astype(np.float64) - e) <= asum * 2.0 ** -16 + 1e-30).all()
+        elif c == "v1_mean":
+            assert (np.abs(g.astype(np.float64) - e) <= asum / cnt * 2.0 ** -16 + 1e-30).all()
+        else:
+            np.testing.assert_array_equal(g, e, err_msg=c)
+
+
+def test_groupby_float_keys_nan_groups(P):
+    rng = np.random.default_rng(9)
+    n = 10_000
+    k = rng.integers(0, 20, n).astype(np.float32)
+    k[rng.integers(0, n, 50)] = np.nan
+    k[rng.integers(0, n, 50)] = -0.0
+    v = rng.integers(0, 100, n).astype(np.int32)
+    uk, out = P.groupby_aggregate(k, {"v": v}, {"v": "sum"})
+    ek, eout = O.groupby_aggregate(k, {"v": v}, {"v": "sum"})
+    np.testing.assert_array_equal(_np(uk).view(np.uint32), ek.view(np.uint32))
+    np.testing.assert_array_equal(_np(out["v"]), eout["v"])
+
+
+def test_groupby_all_equal_and_heavy(P):
+    n = 300_000
+    k = np.full(n, 7, dtype=np.int64)
+    v = np.ones(n, dtype=np.float64)
+    uk, out = P.groupby_aggregate(k, {"v": v}, {"v": "sum"})
+    assert _np(uk).tolist() == [7] and _np(out["v"]).tolist() == [float(n)]
+    rng = np.random.default_rng(1)
+    k = rng.integers(0, 1000, n).astype(np.int32)
+    k[rng.random(n) < 0.7] = 3
+    v = rng.integers(-5, 5, n).astype(np.int64)
+    uk, out = P.groupby_aggregate(k, {"v": v}, {"v": "max"})
+    ek, eout = O.groupby_aggregate(k, {"v": v}, {"v": "max"})
+    np.testing.assert_array_equal(_np(uk), ek)
+    np.testing.assert_array_equal(_np(out["v"]), eout["v"])
+
+
+# -------------------------------------------------------------------- join ---
+@pytest.mark.parametrize("nl,nr,kr", [(1, 1, 2), (100, 50, 20), (10_000, 5_000, 3000), (200_000, 100_000, 50_000),
+                                      (5_000, 7, 3)])
+def test_inner_join_pairs(P, nl, nr, kr):
+    rng = np.random.default_rng(nl + nr)
+    lk = rng.integers(0, kr, nl).astype(np.int64)
+    rk = rng.integers(0, kr, nr).astype(np.int64)
+    j = P.ParallelSortMergeJoin()
+    mk, li, ri = j.join_indices(lk, rk, "inner")
+    eli, eri, sl, pl, sr, pr = O.inner_join_pairs(lk, rk)
+    np.testing.assert_array_equal(_np(li), pl[eli])
+    np.testing.assert_array_equal(_np(ri), pr[eri])
+    np.testing.assert_array_equal(_np(mk), sl[eli])
+
+
+def test_join_c2_like_payloads(P):
+    rng = np.random.default_rng(42 + 1)
+    nl, nr = 1_000_000, 500_000
+    lk = rng.integers(0, nr, nl).astype(np.int64)
+    lv = rng.standard_normal(nl).astype(np.float32)
+    rk = rng.permutation(nr).astype(np.int64)
+    rv = rng.integers(-2**31, 2**31, nr).astype(np.int32)
+    mk, out = P.sort_merge_join(lk, {"lv": lv}, rk, {"rv": rv}, "inner")
+    emk, eout, _, _ = O.sort_merge_join(lk, {"lv": lv}, rk, {"rv": rv}, "inner")
+    np.testing.assert_array_equal(_np(mk), emk)
+    for c in eout:
+        g = _np(out[c])
+        assert g.dtype == eout[c].dtype
+        np.testing.assert_array_equal(g, eout[c])
+
+
+@pytest.mark.parametrize("how", ["left", "right", "outer"])
+def test_non_inner_joins(P, how):
+    rng = np.random.default_rng(len(how))
+    for nl, nr in [(1, 1), (50, 80), (20_000, 9_000)]:
+        lk = rng.integers(0, 60, nl).astype(np.int32)
+        rk = rng.integers(20, 90, nr).astype(np.int32)
+        lv = rng.integers(0, 100, nl).astype(np.int32)
+        rv = rng.standard_normal(nr).astype(np.float32)
+        mk, out = P.sort_merge_join(lk, {"a": lv}, rk, {"b": rv}, how)
+        emk, eout, _, _ = O.sort_merge_join(lk, {"a": lv}, rk, {"b": rv}, how)
+        np.testing.assert_array_equal(_np(mk), emk)
+        for c in eout:
+            np.testing.assert_array_equal(_np(out[c]), eout[c], err_msg=f"{how} {c}")
+
+
+# --------------------------------------------------------------- partition ---
+@pytest.mark.parametrize("p", [1, 7, 256, 2048])
+def test_hash_partition(P, p):
+    rng = np.random.default_rng(p)
+    for n in [1, 1000, 300_001]:
+        k1 = rng.integers(-2**31, 2**31, n).astype(np.int32)
+        k2 = rng.integers(0, 100, n).astype(np.int64)
+        for keys in ([k1], [k1, k2]):
+            t, perm, offs = P.hash_partition(keys, p)
+            et, ep, eo = O.hash_partition(keys, p)
+            np.testing.assert_array_equal(_np(t), et)
+            np.testing.assert_array_equal(_np(perm), ep)
+            np.testing.assert_array_equal(_np(offs), eo)
+
+
+def test_hash_values_all_dtypes(P):
+    rng = np.random.default_rng(3)
+    n = 5000
+    cols = [rng.integers(-100, 100, n).astype(np.int8), rng.integers(-2**15, 2**15, n).astype(np.int16),
+            rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32), rng.integers(-2**40, 2**40, n),
+            rng.standard_normal(n).astype(np.float32), rng.standard_normal(n)]
+    for c in cols:
+        if c.dtype == np.float64:
+            continue  # single float64 key: 2 words per row (covered below)
+        np.testing.assert_array_equal(_np(P.hash_multi_columns([c])), O.hash_multi_columns([c]))
+    np.testing.assert_array_equal(_np(P.hash_multi_columns(cols)), O.hash_multi_columns(cols))
+    np.testing.assert_array_equal(_np(P.hash_multi_columns([cols[-1]])), O.hash_multi_columns([cols[-1]]))
