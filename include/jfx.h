@@ -110,27 +110,44 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key,
                 const jfx_agg_column* values, int nvalues, void* const* unique_out,
                 int64_t* num_groups, void* workspace, size_t workspace_bytes, void* stream);
 
-/* Opaque state passed from jfx_join_prepare to jfx_join_expand (caller-owned,
- * plain memory; it points into the workspace, which must stay untouched). */
+/* Opaque state passed from jfx_join_prepare to the other join calls
+ * (caller-owned plain memory; it points into the workspace, which must stay
+ * untouched until the last call that uses the plan). */
 typedef struct {
-  uint64_t opaque[64];
+  uint64_t opaque[160];
 } jfx_join_plan;
 
-/* ParallelSortMergeJoin.join (:938-1075), first half: radix sorts both key
- * columns with one shared key packing and counts the output rows for `how`
- * (JFX_JOIN_INNER / LEFT / RIGHT).  *num_out receives the row count after one
- * stream synchronisation. */
-int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* right_key,
-                     int64_t nr, int how, jfx_join_plan* plan, int64_t* num_out,
+/* ParallelSortMergeJoin.join (:938-1075) and join_multi_column (:826-936),
+ * first half: radix sorts both sides by their ncols key columns under one
+ * shared key packing and counts, for every row of the driving side, its
+ * equal-key run on the other side.  `how`: JFX_JOIN_INNER / LEFT / RIGHT /
+ * OUTER (OUTER = inner pairs plus the counts needed for both sides' unmatched
+ * rows).  *num_out receives the row count jfx_join_expand writes (inner pairs
+ * for INNER/OUTER, one row per left/right row for LEFT/RIGHT) after one stream
+ * synchronisation. */
+int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys,
+                     int64_t nr, int ncols, int how, jfx_join_plan* plan, int64_t* num_out,
                      void* workspace, size_t workspace_bytes, void* stream);
 
 /* Second half: writes num_out rows of (left row id, right row id) -- -1 for a
- * missing side -- and, if keys_out is non-null, the merged key column (key
- * dtype).  Row order is the reference's: inner pairs by (key, left row, right
- * row); left/right rows in that side's sorted order with the first match of
- * the other side. */
+ * missing side -- and, for each non-null keys_out[c], the key column c of the
+ * driving side.  Row order is the reference's sorted merge order: inner pairs
+ * by (key, left row, right row); left/right rows in that side's sorted order
+ * with the first match of the other side (searchsorted, :1013-1034). */
 int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out,
-                    void* keys_out, void* stream);
+                    void* const* keys_out, void* stream);
+
+/* Rows of one side (0 = left, 1 = right) that have no match, in ascending row
+ * order, as join_multi_column appends them (:883-917).  *count receives the
+ * number after one stream synchronisation; rows_out needs that capacity. */
+int jfx_join_unmatched(const jfx_join_plan* plan, int side, int32_t* rows_out, int64_t capacity,
+                       int64_t* count, void* stream);
+
+/* _coalesce_join_key (:1245-1251): out[i] = left[left_idx[i]] when
+ * left_idx[i] >= 0, else right[right_idx[i]] (both columns of `dtype`). */
+int jfx_coalesce(const void* left, const int32_t* left_idx, int64_t nl, const void* right,
+                 const int32_t* right_idx, int64_t nr, int64_t n, int32_t dtype, void* out,
+                 void* stream);
 
 /* Payload gather with the reference's join fill (:1056-1073): out[i] =
  * src[idx[i]] converted to out_dtype, NaN where idx[i] < 0 (float outputs). */

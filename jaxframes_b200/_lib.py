@@ -60,7 +60,7 @@ class AggColumn(ctypes.Structure):
 
 
 class JoinPlan(ctypes.Structure):
-    _fields_ = [("opaque", ctypes.c_uint64 * 64)]
+    _fields_ = [("opaque", ctypes.c_uint64 * 160)]
 
 
 _P = ctypes.c_void_p
@@ -78,9 +78,11 @@ SIGNATURES = {
     "jfx_lexsort": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P, _SIZE, _P]),
     "jfx_groupby": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, ctypes.POINTER(AggColumn), _INT,
                            ctypes.POINTER(_P), ctypes.POINTER(_I64), _P, _SIZE, _P]),
-    "jfx_join_prepare": (_INT, [ctypes.POINTER(Column), _I64, ctypes.POINTER(Column), _I64, _INT,
+    "jfx_join_prepare": (_INT, [ctypes.POINTER(Column), _I64, ctypes.POINTER(Column), _I64, _INT, _INT,
                                 ctypes.POINTER(JoinPlan), ctypes.POINTER(_I64), _P, _SIZE, _P]),
-    "jfx_join_expand": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, _P, _P]),
+    "jfx_join_expand": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, ctypes.POINTER(_P), _P]),
+    "jfx_join_unmatched": (_INT, [ctypes.POINTER(JoinPlan), _INT, _P, _I64, ctypes.POINTER(_I64), _P]),
+    "jfx_coalesce": (_INT, [_P, _P, _I64, _P, _P, _I64, _I64, ctypes.c_int32, _P, _P]),
     "jfx_gather": (_INT, [_P, ctypes.c_int32, _I64, _P, _I64, _P, ctypes.c_int32, _P]),
     "jfx_hash_columns": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P]),
     "jfx_hash_partition": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, _P, _P, _P, _P, _SIZE, _P]),

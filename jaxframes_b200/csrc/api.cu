@@ -111,26 +111,32 @@ struct JoinPlan {
   u64 magic;
   int how;
   int key64;
-  int dtype;
-  u32 flags;
-  u64 tmin;
+  int ncols;
+  int reverse_counted;  // counts with the sides swapped exist (lo2/cnt2)
   u64 nl, nr, m;
-  const void* lkey;
-  const void* rkey;
+  u64 unmatched[2];     // rows without a match: [0] left, [1] right
   void* skL;
   void* skR;
   u32* pL;
   u32* pR;
   u32* lo;
   u32* cnt;
+  u32* lo2;
+  u32* cnt2;
   u64* off;
+  u32* flag;
+  u32* foff;
+  u32* fpart;
+  u32* ftotal;
+  ColDesc lc[kMaxCols];
+  ColDesc rc[kMaxCols];
 };
 static_assert(sizeof(JoinPlan) <= sizeof(jfx_join_plan), "join plan does not fit");
-constexpr u64 kJoinMagic = 0x6a66786a6f696e31ull;
+constexpr u64 kJoinMagic = 0x6a66786a6f696e32ull;
 
 struct JoinBuffers {
   void *skL, *skR;
-  u32 *pL, *pR, *lo, *cnt;
+  u32 *pL, *pR, *lo, *cnt, *lo2, *cnt2, *flag, *foff, *fpart, *ftotal;
   u64 *off, *partial, *total;
 };
 static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
@@ -143,9 +149,30 @@ static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, Joi
   j.pR = ar.take<u32>(nr ? nr : 1);
   j.lo = ar.take<u32>(nmax ? nmax : 1);
   j.cnt = ar.take<u32>(nmax ? nmax : 1);
+  j.lo2 = ar.take<u32>(nmax ? nmax : 1);
+  j.cnt2 = ar.take<u32>(nmax ? nmax : 1);
   j.off = ar.take<u64>(nmax ? nmax : 1);
   j.partial = ar.take<u64>(scan_partials_count(nmax));
   j.total = ar.take<u64>(4);
+  j.flag = ar.take<u32>(nmax ? nmax : 1);
+  j.foff = ar.take<u32>(nmax ? nmax : 1);
+  j.fpart = ar.take<u32>(scan_partials_count(nmax));
+  j.ftotal = ar.take<u32>(4);
+}
+
+template <typename K>
+static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* lo, u32* cnt, const PackDesc& pd,
+                             cudaStream_t s) {
+  if (!na) return JFX_OK;
+  if (!nb) {
+    JFX_CUDA(cudaMemsetAsync(cnt, 0, na * sizeof(u32), s));
+    JFX_CUDA(cudaMemsetAsync(lo, 0, na * sizeof(u32), s));
+    return JFX_OK;
+  }
+  const unsigned blocks = (unsigned)((na + kJoinTile - 1) / kJoinTile);
+  k_join_count<K><<<blocks, kJoinThreads, 0, s>>>((const K*)A, na, (const K*)B, nb, lo, cnt, pd), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
 }
 
 // -------------------------------------------------------------- partition ---
@@ -440,17 +467,21 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   return JFX_OK;
 }
 
-int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* right_key, int64_t nr, int how,
-                     jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
+int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys, int64_t nr, int ncols,
+                     int how, jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
                      void* stream) {
   JFX_TRY(check_n(nl));
   JFX_TRY(check_n(nr));
-  if (!left_key || !right_key || !plan_out || !num_out) return fail(JFX_ERR_ARG, "null argument");
-  if (left_key->dtype != right_key->dtype)
-    return fail(JFX_ERR_DTYPE, "join keys must share a dtype (got %d and %d)", left_key->dtype, right_key->dtype);
-  if (left_key->dtype == JFX_BOOL) return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
-  if (how != JFX_JOIN_INNER && how != JFX_JOIN_LEFT && how != JFX_JOIN_RIGHT)
-    return fail(JFX_ERR_ARG, "join kind %d is not supported by this entry point", how);
+  if (!left_keys || !right_keys || !plan_out || !num_out) return fail(JFX_ERR_ARG, "null argument");
+  if (ncols < 1 || ncols > kMaxCols) return fail(JFX_ERR_ARG, "1..%d join key columns supported", kMaxCols);
+  for (int c = 0; c < ncols; ++c) {
+    if (left_keys[c].dtype != right_keys[c].dtype)
+      return fail(JFX_ERR_DTYPE, "join key %d: left and right dtypes differ (%d, %d)", c, left_keys[c].dtype,
+                  right_keys[c].dtype);
+    if (ncols == 1 && left_keys[c].dtype == JFX_BOOL)
+      return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
+  }
+  if (how < JFX_JOIN_INNER || how > JFX_JOIN_OUTER) return fail(JFX_ERR_ARG, "unknown join kind %d", how);
   cudaStream_t s = as_stream(stream);
   Arena ar(workspace, workspace_bytes);
   Common c;
@@ -459,27 +490,36 @@ int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* r
   carve_join(ar, (u64)nl, (u64)nr, c, b, j);
   if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  // a single key is sorted by ParallelRadixSort (narrow ints keep the
+  // reference's unsigned order); several keys are compared for equality only
+  const u32 flags = ncols == 1 ? CF_QUIRK : 0u;
   PackDesc pl, pr;
-  JFX_TRY(build_pack(left_key, 1, CF_QUIRK, false, pl));
-  JFX_TRY(build_pack(right_key, 1, CF_QUIRK, false, pr));
-  // shared packing: min and max over both sides
+  JFX_TRY(build_pack(left_keys, ncols, flags, false, pl));
+  JFX_TRY(build_pack(right_keys, ncols, flags, false, pr));
+  // shared packing: min and max of every column over both sides
   JFX_TRY(launch_minmax(pl, (u64)nl, c.mm, s));
-  JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2, s));
+  JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2 * kMaxCols, s));
   u64* host = g_host.get();
-  JFX_TRY(read_back(c.mm, 4 * sizeof(u64), host, s));
-  u64 mn = std::min(host[0], host[2]), mx = 0;
-  if (nl) mx = std::max(mx, host[1]);
-  if (nr) mx = std::max(mx, host[3]);
-  if (!nl && !nr) mn = 0;
-  const int bits = bit_length(mx - mn);
-  pl.c[0].tmin = pr.c[0].tmin = mn;
-  pl.c[0].bits = pr.c[0].bits = bits;
-  pl.c[0].shift = pr.c[0].shift = 0;
-  const bool key64 = bits > 32;
+  JFX_TRY(read_back(c.mm, 4 * kMaxCols * sizeof(u64), host, s));
+  int shift = 0;
+  for (int k = ncols - 1; k >= 0; --k) {
+    u64 mn = ~0ull, mx = 0;
+    if (nl) { mn = std::min(mn, host[2 * k]); mx = std::max(mx, host[2 * k + 1]); }
+    if (nr) { mn = std::min(mn, host[2 * kMaxCols + 2 * k]); mx = std::max(mx, host[2 * kMaxCols + 2 * k + 1]); }
+    if (!nl && !nr) mn = mx = 0;
+    const int bits = bit_length(mx - mn);
+    pl.c[k].tmin = pr.c[k].tmin = mn;
+    pl.c[k].bits = pr.c[k].bits = bits;
+    pl.c[k].shift = pr.c[k].shift = shift;
+    shift += bits;
+  }
+  if (shift > 64) return fail(JFX_ERR_CAPACITY, "join keys need %d packed bits; at most 64 are supported", shift);
+  const int total_bits = shift;
+  const bool key64 = total_bits > 32;
   if (nl) {
     RadixRequest rq;
     rq.pack = pl;
-    rq.total_bits = bits;
+    rq.total_bits = total_bits;
     rq.key64 = key64;
     rq.perm_out = j.pL;
     rq.keys_out = j.skL;
@@ -488,74 +528,68 @@ int jfx_join_prepare(const jfx_column* left_key, int64_t nl, const jfx_column* r
   if (nr) {
     RadixRequest rq;
     rq.pack = pr;
-    rq.total_bits = bits;
+    rq.total_bits = total_bits;
     rq.key64 = key64;
     rq.perm_out = j.pR;
     rq.keys_out = j.skR;
     JFX_TRY(radix_sort(rq, (u64)nr, b, c.err, s));
   }
-  const int nan_key = dtype_is_float(left_key->dtype);
-  const u64 nant = left_key->dtype == JFX_F32 ? (u64)kF32NanT : kF64NanT;
-  const u64 nan_packed = nant - mn;
-  // count: A = the side whose rows drive the output
+  // forward counts drive inner/left joins, swapped counts right joins; the
+  // unmatched rows of a side need that side's counts
   const bool swap = how == JFX_JOIN_RIGHT;
   const u64 na = swap ? nr : nl, nb = swap ? nl : nr;
   const void* A = swap ? j.skR : j.skL;
   const void* B = swap ? j.skL : j.skR;
-  u64 m = 0;
-  if (na && nb) {
-    const unsigned blocks = (unsigned)((na + kJoinTile - 1) / kJoinTile);
-    if (key64)
-      k_join_count<u64><<<blocks, kJoinThreads, 0, s>>>((const u64*)A, na, (const u64*)B, nb, j.lo, j.cnt, nan_key, (u64)nan_packed), note_launch();
-    else
-      k_join_count<u32><<<blocks, kJoinThreads, 0, s>>>((const u32*)A, na, (const u32*)B, nb, j.lo, j.cnt, nan_key, (u32)nan_packed), note_launch();
-    JFX_CUDA(cudaGetLastError());
-  } else if (na) {
-    JFX_CUDA(cudaMemsetAsync(j.cnt, 0, na * sizeof(u32), s));
-    JFX_CUDA(cudaMemsetAsync(j.lo, 0, na * sizeof(u32), s));
+  if (key64) JFX_TRY(launch_join_count<u64>(A, na, B, nb, j.lo, j.cnt, pl, s));
+  else JFX_TRY(launch_join_count<u32>(A, na, B, nb, j.lo, j.cnt, pl, s));
+  const bool rev = how == JFX_JOIN_OUTER;
+  if (rev) {
+    if (key64) JFX_TRY(launch_join_count<u64>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, s));
+    else JFX_TRY(launch_join_count<u32>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, s));
   }
-  if (how == JFX_JOIN_INNER) {
-    if (na && nb) {
-      JFX_TRY(device_exclusive_scan<u64>(j.cnt, na, j.off, j.total, j.partial, s));
-      JFX_CUDA(cudaMemcpyAsync(host + 1, j.total, sizeof(u64), cudaMemcpyDeviceToHost, s));
-    } else {
-      host[1] = 0;
-    }
+  host[1] = 0;
+  if (na && nb) {
+    JFX_TRY(device_exclusive_scan<u64>(j.cnt, na, j.off, j.total, j.partial, s));
+    JFX_CUDA(cudaMemcpyAsync(host + 1, j.total, sizeof(u64), cudaMemcpyDeviceToHost, s));
   }
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaStreamSynchronize(s));
   JFX_TRY(check_err_word((u32)host[0]));
-  if (how == JFX_JOIN_INNER) {
-    m = (na && nb) ? host[1] : 0;
-    if (m > (u64)0x7fffffffull) return fail(JFX_ERR_CAPACITY, "inner join produces %llu rows; at most 2^31-1 are supported", m);
-  } else {
-    m = na;
-  }
+  const u64 inner = (na && nb) ? host[1] : 0;
+  u64 m = how == JFX_JOIN_INNER || how == JFX_JOIN_OUTER ? inner : na;
+  if (m > (u64)0x7fffffffull) return fail(JFX_ERR_CAPACITY, "join produces %llu rows; at most 2^31-1 are supported", m);
   JoinPlan* jp = (JoinPlan*)plan_out;
   memset(plan_out, 0, sizeof *plan_out);
   jp->magic = kJoinMagic;
   jp->how = how;
   jp->key64 = key64;
-  jp->dtype = left_key->dtype;
-  jp->flags = CF_QUIRK;
-  jp->tmin = mn;
+  jp->ncols = ncols;
+  jp->reverse_counted = rev;
   jp->nl = (u64)nl;
   jp->nr = (u64)nr;
   jp->m = m;
-  jp->lkey = left_key->data;
-  jp->rkey = right_key->data;
   jp->skL = j.skL;
   jp->skR = j.skR;
   jp->pL = j.pL;
   jp->pR = j.pR;
   jp->lo = j.lo;
   jp->cnt = j.cnt;
+  jp->lo2 = j.lo2;
+  jp->cnt2 = j.cnt2;
   jp->off = j.off;
+  jp->flag = j.flag;
+  jp->foff = j.foff;
+  jp->fpart = j.fpart;
+  jp->ftotal = j.ftotal;
+  for (int k = 0; k < ncols; ++k) {
+    jp->lc[k] = pl.c[k];
+    jp->rc[k] = pr.c[k];
+  }
   *num_out = (int64_t)m;
   return JFX_OK;
 }
 
-int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out, void* keys_out,
+int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out, void* const* keys_out,
                     void* stream) {
   if (!plan) return fail(JFX_ERR_ARG, "null plan");
   const JoinPlan* jp = (const JoinPlan*)plan;
@@ -565,18 +599,19 @@ int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* r
   cudaStream_t s = as_stream(stream);
   const bool swap = jp->how == JFX_JOIN_RIGHT;
   JoinKeyOut ko;
-  ko.keys_out = keys_out;
-  ko.dtype = jp->dtype;
-  ko.flags = jp->flags;
-  ko.tmin = jp->tmin;
-  ko.orig = swap ? jp->rkey : jp->lkey;
+  memset(&ko, 0, sizeof ko);
+  ko.ncols = jp->ncols;
+  for (int k = 0; k < jp->ncols; ++k) {
+    ko.out[k] = keys_out ? keys_out[k] : nullptr;
+    ko.c[k] = swap ? jp->rc[k] : jp->lc[k];
+  }
   const u64 na = swap ? jp->nr : jp->nl;
   const void* skA = swap ? jp->skR : jp->skL;
   const u32* pA = swap ? jp->pR : jp->pL;
   const u32* pB = swap ? jp->pL : jp->pR;
   int32_t* a_out = swap ? right_idx_out : left_idx_out;
   int32_t* b_out = swap ? left_idx_out : right_idx_out;
-  if (jp->how == JFX_JOIN_INNER) {
+  if (jp->how == JFX_JOIN_INNER || jp->how == JFX_JOIN_OUTER) {
     const unsigned blocks = (unsigned)((jp->m + kJoinTile - 1) / kJoinTile);
     if (jp->key64)
       k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko), note_launch();
@@ -589,6 +624,62 @@ int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* r
     else
       k_join_expand_first<u32><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u32*)skA, a_out, b_out, ko), note_launch();
   }
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+int jfx_join_unmatched(const jfx_join_plan* plan, int side, int32_t* rows_out, int64_t capacity, int64_t* count,
+                       void* stream) {
+  if (!plan || !count) return fail(JFX_ERR_ARG, "null argument");
+  const JoinPlan* jp = (const JoinPlan*)plan;
+  if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
+  if (side != 0 && side != 1) return fail(JFX_ERR_ARG, "side must be 0 (left) or 1 (right)");
+  const u32 *cnt, *pA;
+  u64 na;
+  if (side == 0) {
+    if (jp->how == JFX_JOIN_RIGHT) return fail(JFX_ERR_ARG, "a right-join plan holds no counts for left rows");
+    cnt = jp->cnt;
+    pA = jp->pL;
+    na = jp->nl;
+  } else if (jp->how == JFX_JOIN_RIGHT) {
+    cnt = jp->cnt;
+    pA = jp->pR;
+    na = jp->nr;
+  } else if (jp->reverse_counted) {
+    cnt = jp->cnt2;
+    pA = jp->pR;
+    na = jp->nr;
+  } else {
+    return fail(JFX_ERR_ARG, "right rows' counts exist only for right/outer plans");
+  }
+  *count = 0;
+  if (!na) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  const int g = grid_for(na, 256);
+  k_mark_unmatched<<<g, 256, 0, s>>>(cnt, pA, na, jp->flag), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  JFX_TRY(device_exclusive_scan<u32>(jp->flag, na, jp->foff, jp->ftotal, jp->fpart, s));
+  u64* host = g_host.get();
+  JFX_CUDA(cudaMemcpyAsync(host, jp->ftotal, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  const u64 k = (u32)host[0];
+  *count = (int64_t)k;
+  if (k > (u64)capacity || (!rows_out && k)) return fail(JFX_ERR_CAPACITY, "%llu unmatched rows exceed capacity %lld", k, (long long)capacity);
+  if (k) {
+    k_compact_rows<<<g, 256, 0, s>>>(jp->flag, jp->foff, na, rows_out), note_launch();
+    JFX_CUDA(cudaGetLastError());
+  }
+  return JFX_OK;
+}
+
+int jfx_coalesce(const void* left, const int32_t* left_idx, int64_t nl, const void* right, const int32_t* right_idx,
+                 int64_t nr, int64_t n, int32_t dtype, void* out, void* stream) {
+  if (n < 0 || nl < 0 || nr < 0) return fail(JFX_ERR_ARG, "negative count");
+  if (n == 0) return JFX_OK;
+  if (!left_idx || !right_idx || !out) return fail(JFX_ERR_ARG, "null pointer");
+  if (dtype_size(dtype) == 0) return fail(JFX_ERR_DTYPE, "unsupported dtype");
+  cudaStream_t s = as_stream(stream);
+  k_coalesce<<<grid_for((u64)n, 256), 256, 0, s>>>(left, left_idx, (u64)nl, right, right_idx, (u64)nr, (u64)n, dtype, out), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }

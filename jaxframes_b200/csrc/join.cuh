@@ -41,8 +41,7 @@ __device__ __forceinline__ u64 upper_bound_g(const K* a, u64 lo, u64 hi, K x) {
 // of B keys equal to A[i] (0 for a NaN key, which equals nothing).
 template <typename K>
 __global__ void __launch_bounds__(kJoinThreads) k_join_count(const K* A, u64 na, const K* B, u64 nb,
-                                                            u32* lo_out, u32* cnt_out, int nan_key,
-                                                            K nan_packed) {
+                                                            u32* lo_out, u32* cnt_out, PackDesc pd) {
   constexpr int CAP = (32 * 1024) / sizeof(K);
   __shared__ K win[CAP];
   __shared__ u64 wlo_s, whi_s;
@@ -72,25 +71,31 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_count(const K* A, u64 na,
       h = upper_bound_g<K>(B + wlo, l, wn, x);
     }
     u32 c = (u32)(h - l);
-    if (nan_key && x == nan_packed) c = 0;
+    if (pd.nan_cols && packed_has_nan<K>(pd, x)) c = 0;
     lo_out[i] = (u32)(wlo + l);
     cnt_out[i] = c;
   }
 }
 
+// Merged key columns written by the expand kernels (A side's key values).
 struct JoinKeyOut {
-  void* keys_out;    // merged key column (dtype of the A side key), or null
-  int dtype;
-  u32 flags;
-  u64 tmin;
-  const void* orig;  // original A key column (float keys are gathered from it)
+  int ncols;
+  void* out[kMaxCols];  // per column output, or null
+  ColDesc c[kMaxCols];  // A side's columns with the shared packing
 };
 
 template <typename K>
 __device__ __forceinline__ void write_join_key(const JoinKeyOut& ko, u64 o, K packed, u32 row) {
-  if (!ko.keys_out) return;
-  if (dtype_is_float(ko.dtype)) store_raw(ko.keys_out, ko.dtype, o, load_raw(ko.orig, ko.dtype, row));
-  else store_raw(ko.keys_out, ko.dtype, o, untransform_int(ko.dtype, ko.flags, (u64)packed + ko.tmin));
+  for (int j = 0; j < ko.ncols; ++j) {
+    if (!ko.out[j]) continue;
+    const ColDesc& c = ko.c[j];
+    if (dtype_is_float(c.dtype)) {
+      store_raw(ko.out[j], c.dtype, o, load_raw(c.ptr, c.dtype, row));
+    } else {
+      const u64 field = c.bits ? (((u64)packed >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull))) : 0ull;
+      store_raw(ko.out[j], c.dtype, o, untransform_int(c.dtype, c.flags, field + c.tmin));
+    }
+  }
 }
 
 // Inner join: output o belongs to the sorted A row i with off[i] <= o < off[i+1].
@@ -191,6 +196,34 @@ __global__ void __launch_bounds__(256) k_gather(const void* src, int sdt, u64 n_
     } else {
       store_raw(out, odt, i, (u64)(long long)x);
     }
+  }
+}
+
+// flag[pA[i]] = 1 for sorted A rows without a match (original row order).
+__global__ void __launch_bounds__(256) k_mark_unmatched(const u32* cnt, const u32* pA, u64 na, u32* flag) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (u64)gridDim.x * blockDim.x)
+    flag[pA[i]] = cnt[i] == 0 ? 1u : 0u;
+}
+
+// out[off[r]] = r for every flagged row r (stable compaction).
+__global__ void __launch_bounds__(256) k_compact_rows(const u32* flag, const u32* off, u64 n, int32_t* out) {
+  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (u64)gridDim.x * blockDim.x)
+    if (flag[r]) out[off[r]] = (int32_t)r;
+}
+
+// _coalesce_join_key (parallel_algorithms.py:1245-1251): left key when the
+// left index is valid, else the right key.
+__global__ void __launch_bounds__(256) k_coalesce(const void* a, const int32_t* ia, u64 na, const void* b,
+                                                 const int32_t* ib, u64 nb, u64 n, int dt, void* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const int32_t x = ia[i];
+    u64 v = 0;
+    if (x >= 0 && (u64)x < na) v = load_raw(a, dt, x);
+    else {
+      const int32_t y = ib[i] < 0 ? 0 : ib[i];
+      if ((u64)y < nb) v = load_raw(b, dt, y);
+    }
+    store_raw(out, dt, i, v);
   }
 }
 

@@ -371,6 +371,73 @@ class SortBasedGroupBy:
         return dict(zip(key_names, uniq)), out
 
 
+def _join_prepare(lcols, rcols, how: str):
+    """jfx_join_prepare: returns (plan, num_out, workspace); the workspace must
+    outlive every later call that uses the plan."""
+    L = _lib.lib()
+    nl, nr = lcols[0].numel(), rcols[0].numel()
+    ws = _lib.workspace(_lib.WS_JOIN, nl, nr, device=lcols[0].device)
+    plan = _lib.JoinPlan()
+    m = ctypes.c_int64(0)
+    la = (_lib.Column * len(lcols))(*[_lib.column(c) for c in lcols])
+    ra = (_lib.Column * len(rcols))(*[_lib.column(c) for c in rcols])
+    check(L.jfx_join_prepare(la, nl, ra, nr, len(lcols), _lib.JOIN_KINDS[how], ctypes.byref(plan), ctypes.byref(m),
+                             ws.data_ptr(), ws.numel(), _stream()))
+    return plan, m.value, ws
+
+
+def _join_expand(plan, m, like, key_cols=None):
+    L = _lib.lib()
+    li = _empty(m, torch.int32, like)
+    ri = _empty(m, torch.int32, like)
+    outs = [_empty(m, c.dtype, like) for c in key_cols] if key_cols else []
+    if m:
+        ptrs = (ctypes.c_void_p * max(len(outs), 1))(*[o.data_ptr() for o in outs]) if outs else None
+        check(L.jfx_join_expand(ctypes.byref(plan), li.data_ptr(), ri.data_ptr(), ptrs, _stream()))
+    return li, ri, outs
+
+
+def _join_unmatched(plan, side: int, n: int, like):
+    L = _lib.lib()
+    out = _empty(max(n, 1), torch.int32, like)
+    cnt = ctypes.c_int64(0)
+    check(L.jfx_join_unmatched(ctypes.byref(plan), side, out.data_ptr(), n, ctypes.byref(cnt), _stream()))
+    return out[:cnt.value]
+
+
+def _same_dtypes(lcols, rcols):
+    out_l, out_r = [], []
+    for a, b in zip(lcols, rcols):
+        if a.dtype != b.dtype:
+            t = torch.promote_types(a.dtype, b.dtype)
+            a, b = a.to(t), b.to(t)
+        out_l.append(a)
+        out_r.append(b)
+    return out_l, out_r
+
+
+def _coalesce(left: torch.Tensor, li: torch.Tensor, right: torch.Tensor, ri: torch.Tensor) -> torch.Tensor:
+    """_coalesce_join_key (parallel_algorithms.py:1245-1251)."""
+    if li.numel() == 0:
+        return left[:0]
+    L = _lib.lib()
+    out = _empty(li.numel(), left.dtype, li)
+    check(L.jfx_coalesce(left.data_ptr(), li.data_ptr(), left.numel(), right.data_ptr(), ri.data_ptr(), right.numel(),
+                         li.numel(), _lib.jfx_dtype(left), out.data_ptr(), _stream()))
+    return out
+
+
+def _gather_join_column(arr: torch.Tensor, idx: torch.Tensor, dtype_name: str, all_valid: bool) -> torch.Tensor:
+    """_gather_join_column (parallel_algorithms.py:1254-1278): string codes are
+    filled with -1; with every index valid the column keeps its dtype;
+    otherwise integers and bools become float32 with NaN where missing."""
+    if idx.numel() == 0:
+        return arr[:0]
+    if dtype_name == "string" or all_valid:
+        return _gather(arr, idx)
+    return _gather(arr, idx, arr.dtype if _is_float(arr) else torch.float32)
+
+
 class ParallelSortMergeJoin:
     """parallel_algorithms.py:806-1075."""
 
@@ -379,39 +446,28 @@ class ParallelSortMergeJoin:
         self.sorter = ParallelRadixSort(sharding_spec)
 
     def join_indices(self, left_keys, right_keys, how: str = "inner"):
-        """(merged_keys, left_idx, right_idx) in the reference's row order."""
+        """(merged_keys, left_idx, right_idx) of ``join`` in the reference's row order."""
         if how not in _lib.JOIN_KINDS:
             raise ValueError(f"Unsupported join type: {how}")
-        lk = as_device(left_keys)
-        rk = as_device(right_keys)
-        if lk.dtype != rk.dtype:
-            common = torch.promote_types(lk.dtype, rk.dtype)
-            lk, rk = lk.to(common), rk.to(common)
+        (lk,), (rk,) = _same_dtypes([as_device(left_keys)], [as_device(right_keys)])
         if how == "outer":
             return self._outer_indices(lk, rk)
-        L = _lib.lib()
-        ws = _lib.workspace(_lib.WS_JOIN, lk.numel(), rk.numel(), device=lk.device)
-        plan = _lib.JoinPlan()
-        m = ctypes.c_int64(0)
-        cl, cr = _lib.column(lk), _lib.column(rk)
-        check(L.jfx_join_prepare(ctypes.byref(cl), lk.numel(), ctypes.byref(cr), rk.numel(), _lib.JOIN_KINDS[how],
-                                 ctypes.byref(plan), ctypes.byref(m), ws.data_ptr(), ws.numel(), _stream()))
-        M = m.value
-        li = _empty(M, torch.int32, lk)
-        ri = _empty(M, torch.int32, lk)
-        mk = _empty(M, lk.dtype, lk)
-        if M:
-            check(L.jfx_join_expand(ctypes.byref(plan), li.data_ptr(), ri.data_ptr(), mk.data_ptr(), _stream()))
+        plan, m, ws = _join_prepare([lk], [rk], how)
+        li, ri, (mk,) = _join_expand(plan, m, lk, [rk if how == "right" else lk])
+        del ws
         return mk, li, ri
 
     def _outer_indices(self, lk, rk):
-        # unique keys of both sides (jnp.unique, line 999-1000), then the first
-        # match of each side (searchsorted, line 1003-1046)
-        both = torch.cat([lk, rk])
+        # jnp.unique over both sides (line 999-1000), then the first match of
+        # each side (searchsorted, line 1003-1046)
+        L = _lib.lib()
+        both = _empty(lk.numel() + rk.numel(), lk.dtype, lk)
+        both[: lk.numel()].copy_(lk)
+        both[lk.numel():].copy_(rk)
         uniq, _ = _run_groupby([both], {}, {}, multi=False)
         u = uniq[0]
-        _, ul, li = self.join_indices(u, lk, "left")
-        _, ur, ri = self.join_indices(u, rk, "left")
+        _, _, li = self.join_indices(u, lk, "left")
+        _, _, ri = self.join_indices(u, rk, "left")
         return u, li, ri
 
     def join(self, left_keys, left_values: dict, right_keys, right_values: dict, how: str = "inner"):
@@ -427,6 +483,53 @@ class ParallelSortMergeJoin:
             t = as_device(a)
             out[f"right_{c}"] = _gather(t, ri, t.dtype if _is_float(t) else config.default_float())
         return mk, out
+
+    def join_multi_indices(self, left_keys, right_keys, how: str = "inner"):
+        """Index pairs of ``join_multi_column`` (parallel_algorithms.py:868-917):
+        matches in ORIGINAL row-major order (left row, then right row), then the
+        unmatched left rows (left/outer) and unmatched right rows (right/outer),
+        the missing side being -1."""
+        if how not in _lib.JOIN_KINDS:
+            raise ValueError(f"Unsupported join type: {how}")
+        lcols, rcols = _same_dtypes([as_device(k) for k in left_keys], [as_device(k) for k in right_keys])
+        plan, m, ws = _join_prepare(lcols, rcols, "outer" if how in ("right", "outer") else "inner")
+        li, ri, _ = _join_expand(plan, m, lcols[0])
+        if m:
+            order = multi_column_lexsort([li, ri])
+            li, ri = _gather(li, order), _gather(ri, order)
+        nl, nr = lcols[0].numel(), rcols[0].numel()
+        lun = _join_unmatched(plan, 0, nl, li) if how in ("left", "outer") else li[:0]
+        run = _join_unmatched(plan, 1, nr, li) if how in ("right", "outer") else li[:0]
+        del ws
+        neg = lambda k: torch.full((k,), -1, dtype=torch.int32, device=li.device)
+        if how == "inner":
+            return li, ri
+        if how == "left":
+            return torch.cat([li, lun]), torch.cat([ri, neg(lun.numel())])
+        if how == "right":
+            return torch.cat([li, neg(run.numel())]), torch.cat([ri, run])
+        return (torch.cat([li, lun, neg(run.numel())]), torch.cat([ri, neg(lun.numel()), run]))
+
+    def join_multi_column(self, left_keys, left_key_names, left_values, right_keys, right_key_names, right_values,
+                          how: str = "inner", left_key_dtypes=None, right_key_dtypes=None, left_value_dtypes=None,
+                          right_value_dtypes=None):
+        """Line 826-936: keys coalesced left-first, payloads gathered with -1
+        (string codes) or NaN fill."""
+        li, ri = self.join_multi_indices(left_keys, right_keys, how)
+        lcols, rcols = _same_dtypes([as_device(k) for k in left_keys], [as_device(k) for k in right_keys])
+        l_ok = how in ("inner", "left") or bool((li >= 0).all())
+        r_ok = how in ("inner", "right") or bool((ri >= 0).all())
+        keys = {name: _coalesce(lc, li, rc, ri) for name, lc, rc in zip(left_key_names, lcols, rcols)}
+        vals = {}
+        for name, arr in left_values.items():
+            t = as_device(arr)
+            dn = (left_value_dtypes or {}).get(name, str(t.dtype))
+            vals[f"left_{name}"] = _gather_join_column(t, li, dn, l_ok)
+        for name, arr in right_values.items():
+            t = as_device(arr)
+            dn = (right_value_dtypes or {}).get(name, str(t.dtype))
+            vals[f"right_{name}"] = _gather_join_column(t, ri, dn, r_ok)
+        return keys, vals
 
 
 def _default_spec(sharding_spec):

@@ -143,20 +143,6 @@ def test_lexsort_wide_keys_multi_round(P):
 
 
 # ----------------------------------------------------------------- groupby ---
-def _check_group_outputs(got, exp, vals_sorted_abs_sums=None):
-    for c in exp:
-        g, e = got[c], exp[c]
-        assert g.dtype == e.dtype, (c, g.dtype, e.dtype)
-        if np.issubdtype(e.dtype, np.floating):
-            tol = vals_sorted_abs_sums[c] * 2.0 ** -16 if vals_sorted_abs_sums else 0
-            np.testing.assert_allclose(g.astype(np.float64), e.astype(np.float64), rtol=0, atol=0,
-                                       err_msg=c) if tol is 0 else \
-                np.testing.assert_array_less(np.abs(g.astype(np.float64) - e.astype(np.float64)),
-                                             tol + 1e-30, err_msg=c)
-        else:
-            np.testing.assert_array_equal(g, e, err_msg=c)
-
-
 def _abs_sums_single(keys, v):
     uk, a = O.groupby_aggregate(keys, {"v": np.abs(v.astype(np.float64))}, {"v": "sum"})
     return a["v"]
@@ -295,6 +281,35 @@ def test_non_inner_joins(P, how):
         np.testing.assert_array_equal(_np(mk), emk)
         for c in eout:
             np.testing.assert_array_equal(_np(out[c]), eout[c], err_msg=f"{how} {c}")
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "right", "outer"])
+def test_join_multi_column_original_order(P, how):
+    """join_multi_column pairs in original row-major order plus unmatched rows
+    (parallel_algorithms.py:868-917), against the broadcast-matrix oracle."""
+    rng = np.random.default_rng(7 + len(how))
+    for nl, nr in [(1, 1), (40, 30), (3000, 2000)]:
+        lk = [rng.integers(0, 6, nl).astype(np.int32), rng.integers(0, 5, nl).astype(np.int64)]
+        rk = [rng.integers(2, 8, nr).astype(np.int32), rng.integers(0, 5, nr).astype(np.int64)]
+        li, ri = P.ParallelSortMergeJoin().join_multi_indices(lk, rk, how)
+        eli, eri = O.join_multi_column(lk, rk, how)
+        np.testing.assert_array_equal(_np(li), eli, err_msg=f"{how} {nl}x{nr}")
+        np.testing.assert_array_equal(_np(ri), eri, err_msg=f"{how} {nl}x{nr}")
+
+
+def test_join_multi_column_values(P):
+    lk = [np.array([1, 1, 2], np.int32), np.array([10, 20, 30], np.int32)]
+    rk = [np.array([1, 2], np.int32), np.array([10, 40], np.int32)]
+    keys, vals = P.ParallelSortMergeJoin().join_multi_column(
+        lk, ["a", "b"], {"v": np.array([1, 2, 3], np.int32)}, rk, ["a", "b"], {"w": np.array([4, 5], np.int32)},
+        "left")
+    assert _np(keys["a"]).tolist() == [1, 1, 2] and _np(keys["b"]).tolist() == [10, 20, 30]
+    assert _np(vals["left_v"]).dtype == np.int32  # every left index valid: no promotion
+    w = _np(vals["right_w"])
+    assert w.dtype == np.float32 and w[0] == 4 and np.isnan(w[1:]).all()
+    keys, vals = P.ParallelSortMergeJoin().join_multi_column(
+        lk, ["a", "b"], {}, rk, ["a", "b"], {}, "outer")
+    assert _np(keys["a"]).tolist() == [1, 1, 2, 2] and _np(keys["b"]).tolist() == [10, 20, 30, 40]
 
 
 # --------------------------------------------------------------- partition ---
