@@ -249,6 +249,13 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"workload": "join", "ms_per_step": ms, "value": (NL + NR) / (ms / 1e3)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     # end to end: pinned host buffers in, results back to the host
     h = [torch.from_numpy(x).pin_memory() for x in (lk, lv, rk, rv)]
     h2d = sum(x.numel() * x.element_size() for x in h)
@@ -323,6 +330,50 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_secondary(args):
+    """One secondary config timed alone (used for profiling and tuning)."""
+    import torch
+    torch.cuda.set_device(0)
+    from jaxframes_b200 import build as b
+    b.build()
+    import jaxframes_b200.parallel_algorithms as P
+    dev = torch.device("cuda", 0)
+    if args.workload == "groupby":
+        n = args.n or 100_000_000
+        k1, k2, v1, v2 = [torch.from_numpy(x).to(dev) for x in c3_inputs(n)]
+        vals = {f"v1_{a}": v1 for a in ("sum", "mean", "min", "max", "count")}
+        vals.update({f"v2_{a}": v2 for a in ("sum", "mean", "min", "max", "count")})
+        aggs = {c: c.split("_")[1] for c in vals}
+        fn = lambda: P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)
+        unit_rows = n
+    elif args.workload == "groupby1m":
+        n = args.n or 1_000_000
+        rng = np.random.default_rng(42)
+        k = torch.from_numpy(rng.integers(0, 1000, n).astype(np.int32)).to(dev)
+        v = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+        fn = lambda: P.groupby_aggregate(k, {"v": v, "c": v}, {"v": "sum", "c": "count"})
+        unit_rows = n
+    else:
+        n = args.n or (1 << 28)
+        rng = np.random.default_rng(45)
+        keys = torch.from_numpy(rng.integers(0, 2**63, n, dtype=np.uint64)).to(dev)
+        s = P.ParallelRadixSort()
+        fn = lambda: s.argsort(keys)
+        unit_rows = n
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        fn()
+    b2.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b2) / args.steps
+    print(json.dumps({"workload": args.workload, "rows": n, "ms_per_step": ms, "rows_per_s": unit_rows / (ms / 1e3)}),
+          flush=True)
+
+
 def run_extra(args, P, dev):
     """Secondary measurements on the other configs (not the headline)."""
     import torch
@@ -387,6 +438,10 @@ def main():
     ap.add_argument("--impl", default="jfx", choices=["jfx", "reference"])
     ap.add_argument("--extra", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--workload", default="join", choices=["join", "groupby", "sort", "groupby1m"],
+                    help="join = the headline; the others time one secondary config alone")
+    ap.add_argument("--n", type=int, default=0, help="rows for --workload groupby/sort (0 = config size)")
+    ap.add_argument("--profile", action="store_true", help="timed steps only (no e2e, CPU leg or extras)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -394,6 +449,8 @@ def main():
         if int(os.environ.get("RANK", "0")) != 0:
             return
         run_reference(args)
+    elif args.workload != "join":
+        run_secondary(args)
     else:
         run_gpu(args)
 
