@@ -182,6 +182,54 @@ __device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
   }
 }
 
+// Exclusive prefix of digit d over tiles [0, tile): walks back from tile-1,
+// reading W predecessors' words per round trip, summing aggregates until an
+// inclusive word.  A word not yet published is waited on (bounded).
+template <int W>
+__device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 d, u32 radix, u32* err,
+                                               bool& bad) {
+  u32 excl = 0;
+  long k = (long)tile - 1;  // next predecessor to read
+  while (true) {
+    u32 v[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = (k - i >= 0) ? ld_relaxed(status + (u64)(k - i) * radix + d) : ST_INC;
+    int stop = W;
+    bool found = false;
+    u32 sum = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      const u32 f = v[i] & 0xC0000000u;
+      if (!found && stop == W) {
+        if (f == 0) {
+          stop = i;
+        } else if (f == ST_ERR) {
+          bad = true;
+          found = true;
+        } else {
+          sum += v[i] & ST_CNT;
+          if (f == ST_INC) found = true;
+        }
+      }
+    }
+    excl += sum;
+    if (found) return bad ? 0u : excl;
+    if (stop < W) {
+      const u32 w = wait_status(status + (u64)(k - stop) * radix + d, err);
+      const u32 f = w & 0xC0000000u;
+      if (f == ST_ERR) {
+        bad = true;
+        return 0u;
+      }
+      excl += w & ST_CNT;
+      if (f == ST_INC) return excl;
+      k = k - stop - 1;
+    } else {
+      k -= W;
+    }
+  }
+}
+
 template <typename K, int RB, bool FIRST>
 __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
   using L = PassLayout<K, RB>;
@@ -259,31 +307,15 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   }
   __syncthreads();
 
-  // Publish this tile's counts, then resolve the prefix over earlier tiles.
+  // Publish this tile's counts (tile 0: already inclusive); keep them in sbase.
   u32* st = a.status + (u64)tile * RADIX;
-  for (int d = tid; d < RADIX; d += THREADS)
-    st_relaxed(st + d, (tile == 0 ? ST_INC : ST_AGG) | sexcl[d]);
   for (int d = tid; d < RADIX; d += THREADS) {
-    u32 excl = 0;
-    bool bad = false;
-    if (tile > 0) {
-      const u32* p = a.status + (u64)(tile - 1) * RADIX + d;
-      for (u32 k = tile;; --k) {
-        const u32 v = wait_status(p, a.err);
-        const u32 f = v & 0xC0000000u;
-        if (f == ST_ERR) { bad = true; break; }
-        excl += v & ST_CNT;
-        if (f == ST_INC || k == 1) break;
-        p -= RADIX;
-      }
-      st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + sexcl[d])));
-    }
-    if (bad) sflag[1] = 1u;
-    sbase[d] = a.bin_base[d] + excl;
+    const u32 c = sexcl[d];
+    sbase[d] = c;
+    st_relaxed(st + d, (tile == 0 ? ST_INC : ST_AGG) | c);
   }
-  __syncthreads();
-  if (sflag[1]) return;
-
+  // Tile-local exclusive prefix and shared-memory sort by digit come before
+  // the look-back, which gives earlier tiles time to publish inclusive sums.
   block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);
 
   u32 pos[IPT];
@@ -300,13 +332,29 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
       svals[pos[i]] = val[i];
     }
   }
+
+  // Resolve each digit's prefix over the earlier tiles and publish it.
+  constexpr int W = (RADIX / THREADS) >= 4 ? 8 : 16;
+  for (int d = tid; d < RADIX; d += THREADS) {
+    const u32 c = sbase[d];
+    u32 excl = 0;
+    bool bad = false;
+    if (tile > 0) {
+      excl = lookback_window<W>(a.status, tile, (u32)d, (u32)RADIX, a.err, bad);
+      st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
+    }
+    if (bad) sflag[1] = 1u;
+    // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
+    sbase[d] = a.bin_base[d] + excl - sexcl[d];
+  }
   __syncthreads();
+  if (sflag[1]) return;
 
   K* kout = (K*)a.keys_out;
   for (u32 j = tid; j < tile_n; j += THREADS) {
     const K k = skeys[j];
     const u32 d = digit_of<K>(k, a.digit_mode, a.shift, mask, a.modulus);
-    u64 g = (u64)sbase[d] + (j - sexcl[d]);
+    u64 g = (u64)(u32)(sbase[d] + j);
     if (g >= a.n) {  // only reachable if histogram and pass disagree
       atomicOr(a.err, DERR_BOUNDS);
       continue;
