@@ -63,6 +63,35 @@ def c3_inputs(n=100_000_000, seed=44):
     return k1, k2, v1, v2
 
 
+def c4_keys(nblocks=65_536, block=4096, seed=45):
+    """Skewed uint64 keys: blocks of 4096 assigned by a permutation to 40%
+    floor(lognormal(20, 2)), 40% floored continuous power law (s = 1.2) on
+    [1, 2^40], 20% ascending runs from a uniform start in [0, 2^63) with 5% of
+    positions swapped inside the run."""
+    rng = np.random.default_rng(seed)
+    n_ln = int(nblocks * 0.4)
+    n_zf = int(nblocks * 0.4)
+    n_run = nblocks - n_ln - n_zf
+    kinds = rng.permutation(nblocks)
+    out = np.empty((nblocks, block), dtype=np.uint64)
+    ln = np.floor(rng.lognormal(20.0, 2.0, size=(n_ln, block)))
+    out[kinds[:n_ln]] = np.clip(ln, 0, 2.0 ** 63).astype(np.uint64)
+    s_, m_ = 1.2, 2.0 ** 40
+    u = rng.random((n_zf, block))
+    zf = np.floor((1.0 - u * (1.0 - m_ ** (1.0 - s_))) ** (1.0 / (1.0 - s_)))
+    out[kinds[n_ln:n_ln + n_zf]] = zf.astype(np.uint64)
+    start = rng.integers(0, 2 ** 63, n_run, dtype=np.uint64)
+    runs = start[:, None] + np.arange(block, dtype=np.uint64)[None, :]
+    rows = np.arange(n_run)
+    for _ in range(int(round(0.05 * block))):
+        i = rng.integers(0, block, n_run)
+        j = rng.integers(0, block, n_run)
+        a, b = runs[rows, i].copy(), runs[rows, j].copy()
+        runs[rows, i], runs[rows, j] = b, a
+    out[kinds[n_ln + n_zf:]] = runs
+    return out.reshape(-1)
+
+
 def join_model_bytes(nl, nr, m):
     """Algorithmic bytes of the join: SORT(L) + SORT(R) + merge read + output,
     with K = 8 (int64 key), I = 4, P = ceil(23 / 11) = 3 passes."""
@@ -353,6 +382,27 @@ def run_secondary(args):
         v = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
         fn = lambda: P.groupby_aggregate(k, {"v": v, "c": v}, {"v": "sum", "c": "count"})
         unit_rows = n
+    elif args.workload == "learned":
+        n = args.n or (1 << 28)
+        keys = torch.from_numpy(c4_keys(nblocks=max(1, n // 4096))).to(dev)
+        n = keys.numel()
+        res = {}
+        for mode in ("plain", "learned"):
+            fn = lambda: P.learned_sort(keys, mode=mode)
+            for _ in range(args.warmup):
+                out = fn()
+            torch.cuda.synchronize()
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(args.steps):
+                out = fn()
+            b2.record()
+            torch.cuda.synchronize()
+            res[mode] = {"ms": a.elapsed_time(b2) / args.steps, "learned_used": bool(out[2])}
+        same = bool(torch.equal(P.learned_sort(keys, mode="plain")[1], P.learned_sort(keys, mode="learned")[1]))
+        print(json.dumps({"workload": "learned", "rows": n, **res, "identical_perm": same,
+                          "speedup": res["plain"]["ms"] / res["learned"]["ms"]}), flush=True)
+        return
     else:
         n = args.n or (1 << 28)
         rng = np.random.default_rng(45)
@@ -438,7 +488,7 @@ def main():
     ap.add_argument("--impl", default="jfx", choices=["jfx", "reference"])
     ap.add_argument("--extra", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", default="join", choices=["join", "groupby", "sort", "groupby1m"],
+    ap.add_argument("--workload", default="join", choices=["join", "groupby", "sort", "groupby1m", "learned"],
                     help="join = the headline; the others time one secondary config alone")
     ap.add_argument("--n", type=int, default=0, help="rows for --workload groupby/sort (0 = config size)")
     ap.add_argument("--profile", action="store_true", help="timed steps only (no e2e, CPU leg or extras)")

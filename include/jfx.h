@@ -166,6 +166,20 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
                        int32_t* targets_out, int32_t* perm_out, int64_t* offsets_out,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* Learned-CDF partitioned sort of uint64 keys (no counterpart in the
+ * reference; its output is exactly the plain radix sort's: sorted keys and
+ * the stable int32 permutation).  A 1% strided sample, sorted by the plain
+ * radix sort, trains a two-level piecewise-linear model (root line plus 4096
+ * leaf lines, least squares); radix passes over the model's predicted
+ * position replace the key-digit passes, and runs of equal prediction are
+ * sorted in a fix-up.  mode 0: learned, with the plain sort as fallback when
+ * the model fails its monotonicity check or a run overflows the fix-up;
+ * mode 1: plain radix sort only.  *learned_used (nullable) is 1 when the
+ * learned path produced the result. */
+int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out, int32_t* perm_out,
+                     int mode, int32_t* learned_used, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
 /* Measurement hooks.  No counterpart in the reference, which has no tracing.
  * jfx_launch_count: number of kernels this library has launched so far.
  * jfx_timing_enable(1) clears and starts CUDA-event timing of the radix pass

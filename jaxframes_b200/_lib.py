@@ -86,6 +86,7 @@ SIGNATURES = {
     "jfx_gather": (_INT, [_P, ctypes.c_int32, _I64, _P, _I64, _P, ctypes.c_int32, _P]),
     "jfx_hash_columns": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P]),
     "jfx_hash_partition": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, _P, _P, _P, _P, _SIZE, _P]),
+    "jfx_learned_sort": (_INT, [_P, _I64, _P, _P, _INT, ctypes.POINTER(ctypes.c_int32), _P, _SIZE, _P]),
     "jfx_launch_count": (ctypes.c_uint64, []),
     "jfx_timing_enable": (_INT, [_INT]),
     "jfx_timing_read": (_INT, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I64),

@@ -1,5 +1,6 @@
 // api.cu -- extern "C" entry points of libjfx (declared in include/jfx.h).
 #include "join.cuh"
+#include "learned.cuh"
 
 namespace jfx {
 
@@ -175,6 +176,68 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
   return JFX_OK;
 }
 
+// ---------------------------------------------------------------- learned ---
+struct LearnedBuffers {
+  u64* sample;
+  u64* ssorted;
+  u32* sperm;
+  double* acc;
+  ModelRef* model;
+  Leaf* leaves;
+  u32* first;
+  u32* last;
+  double* fit;
+  u32* flags;  // [0] ok
+  FixLists fix;
+  u64 s, tiles;
+};
+static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBuffers& l) {
+  carve_sort(ar, n, c, b);
+  l.s = n / kSampleStride;
+  l.sample = ar.take<u64>(l.s + 1);
+  l.ssorted = ar.take<u64>(l.s + 1);
+  l.sperm = ar.take<u32>(l.s + 1);
+  l.acc = ar.take<double>(8);
+  l.model = ar.take<ModelRef>(1);
+  l.leaves = ar.take<Leaf>(kLeaves);
+  l.first = ar.take<u32>(kLeaves);
+  l.last = ar.take<u32>(kLeaves);
+  l.fit = ar.take<double>(2 * kLeaves);
+  l.flags = ar.take<u32>(8);
+  l.tiles = (n + kFindTile - 1) / kFindTile;
+  l.fix.cap_small = (u32)(n / 8 + 64);
+  l.fix.cap_medium = (u32)(n / 512 + 64);
+  l.fix.small = ar.take<u32>(2 * (u64)l.fix.cap_small);
+  l.fix.medium = ar.take<u32>(2 * (u64)l.fix.cap_medium);
+  l.fix.counts = ar.take<u32>(8);
+  l.fix.last_start = ar.take<u32>(l.tiles + 1);
+  l.fix.carried_inv = ar.take<u32>(l.tiles + 1);
+}
+
+// Plain radix sort of raw uint64 keys: sorted keys and row ids.
+static int plain_sort_u64(const u64* keys, u64 n, u64* sorted_out, u32* perm_out, SortBuffers& b, Common& c,
+                          cudaStream_t s) {
+  jfx_column col{keys, JFX_U64, 0u};
+  PackDesc pd;
+  JFX_TRY(build_pack(&col, 1, 0u, false, pd));
+  KeyPlan kp;
+  kp.pack = pd;
+  JFX_TRY(plan_keys(kp, n, c.mm, s));
+  RadixRequest rq;
+  rq.pack = kp.pack;
+  rq.total_bits = kp.total_bits;
+  rq.key64 = kp.total_bits > 32;
+  rq.perm_out = perm_out;
+  if (kp.total_bits > 0) {
+    rq.raw_out = sorted_out;
+    rq.raw_dtype = JFX_U64;
+    rq.raw_tmin = kp.pack.c[0].tmin;
+  }
+  JFX_TRY(radix_sort(rq, n, b, c.err, s));
+  if (kp.total_bits == 0) JFX_CUDA(cudaMemcpyAsync(sorted_out, keys, n * 8, cudaMemcpyDeviceToDevice, s));
+  return JFX_OK;
+}
+
 // -------------------------------------------------------------- partition ---
 static void carve_partition(Arena& ar, u64 n, Common& c, SortBuffers& b) { carve_sort(ar, n, c, b); }
 
@@ -247,6 +310,11 @@ size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2) {
     case JFX_WS_PARTITION:
       carve_partition(ar, a, c, b);
       break;
+    case JFX_WS_LEARNED: {
+      LearnedBuffers l;
+      carve_learned(ar, a, c, b, l);
+      break;
+    }
     default:
       return 0;
   }
@@ -277,8 +345,15 @@ int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
   rq.key64 = kp.total_bits > 32;
   rq.reverse = !ascending;
   rq.perm_out = (u32*)perm_out;
+  const bool int_keys = !dtype_is_float(key->dtype);
+  if (sorted_keys_out && int_keys && kp.total_bits > 0) {
+    rq.raw_out = sorted_keys_out;
+    rq.raw_dtype = key->dtype;
+    rq.raw_flags = CF_QUIRK;
+    rq.raw_tmin = kp.pack.c[0].tmin;
+  }
   JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
-  if (sorted_keys_out) {
+  if (sorted_keys_out && !(int_keys && kp.total_bits > 0)) {
     const int g = grid_for((u64)n, 256);
     if (dtype_is_float(key->dtype)) {
       k_gather_same<<<g, 256, 0, s>>>(key->data, key->dtype, (const u32*)perm_out, (u64)n, sorted_keys_out), note_launch();
@@ -745,6 +820,102 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
   u64* host = g_host.get();
   JFX_TRY(read_back(c.err, sizeof(u32), host, s));
   return check_err_word((u32)host[0]);
+}
+
+int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in, int32_t* perm_out, int mode,
+                     int32_t* learned_used, void* workspace, size_t workspace_bytes, void* stream) {
+  JFX_TRY(check_n(n));
+  if (!keys_in || !sorted_out_in || !perm_out) return fail(JFX_ERR_ARG, "null pointer");
+  const u64* keys = (const u64*)keys_in;
+  u64* sorted_keys_out = (u64*)sorted_out_in;
+  if (mode < 0 || mode > 1) return fail(JFX_ERR_ARG, "mode must be 0 (learned, plain fallback) or 1 (plain)");
+  if (learned_used) *learned_used = 0;
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  SortBuffers b;
+  LearnedBuffers l;
+  carve_learned(ar, (u64)n, c, b, l);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  const u64 N = (u64)n;
+  u64* host = g_host.get();
+  if (mode == 1 || N < (1u << 17) || l.s < 4096) {
+    JFX_TRY(plain_sort_u64(keys, N, sorted_keys_out, (u32*)perm_out, b, c, s));
+    JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+    return check_err_word((u32)host[0]);
+  }
+  const int g = grid_for(l.s, 256);
+  // 1. sample and its plain sort (the labels are the sample ranks)
+  k_sample<<<g, 256, 0, s>>>(keys, kSampleStride, l.s, l.sample), note_launch();
+  {
+    jfx_column col{l.sample, JFX_U64, 0u};
+    RadixRequest rq;
+    JFX_TRY(build_pack(&col, 1, 0u, false, rq.pack));
+    rq.pack.c[0].bits = 64;
+    rq.total_bits = 64;
+    rq.key64 = true;
+    rq.perm_out = l.sperm;
+    rq.raw_out = l.ssorted;
+    rq.raw_dtype = JFX_U64;
+    JFX_TRY(radix_sort(rq, l.s, b, c.err, s));
+  }
+  // 2. least-squares fit and the monotonicity check
+  JFX_CUDA(cudaMemsetAsync(l.acc, 0, 8 * sizeof(double), s));
+  k_root_sum<<<g, 256, 0, s>>>(l.ssorted, l.s, l.acc), note_launch();
+  k_root_cov<<<g, 256, 0, s>>>(l.ssorted, l.s, l.acc), note_launch();
+  k_root_solve<<<1, 1, 0, s>>>(l.acc, l.s, l.model, l.leaves), note_launch();
+  JFX_CUDA(cudaMemsetAsync(l.first, 0xff, kLeaves * sizeof(u32), s));
+  JFX_CUDA(cudaMemsetAsync(l.last, 0, kLeaves * sizeof(u32), s));
+  JFX_CUDA(cudaMemsetAsync(l.flags, 0x01, 8 * sizeof(u32), s));
+  k_leaf_bounds<<<g, 256, 0, s>>>(l.ssorted, l.s, l.model, l.first, l.last), note_launch();
+  k_leaf_fit<<<kLeaves * 32 / 256, 256, 0, s>>>(l.ssorted, l.first, l.last, l.fit), note_launch();
+  k_leaf_finalize<<<1, 1024, 0, s>>>(l.ssorted, l.s, N, l.first, l.last, l.fit, l.leaves, l.flags), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  // 3. radix passes over the predicted position
+  {
+    jfx_column col{keys, JFX_U64, 0u};
+    RadixRequest rq;
+    JFX_TRY(build_pack(&col, 1, 0u, false, rq.pack));
+    rq.pack.c[0].bits = 64;
+    rq.digit_mode = DIG_MODEL;
+    rq.model = l.model;
+    rq.total_bits = std::max(1, bit_length(N - 1));
+    rq.key64 = true;
+    rq.perm_out = (u32*)perm_out;
+    rq.keys_out = sorted_keys_out;
+    JFX_TRY(radix_sort(rq, N, b, c.err, s));
+  }
+  // 4. fix-up of runs of equal predicted position
+  JFX_CUDA(cudaMemsetAsync(l.fix.counts, 0, 8 * sizeof(u32), s));
+  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, N, l.model, l.fix), note_launch();
+  k_fix_check<<<grid_for(l.tiles, 256), 256, 0, s>>>(l.tiles, l.fix), note_launch();
+  k_fix_small<<<device_sm_count() * 8, 256, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
+  {
+    static bool attr = false;
+    if (!attr) {
+      JFX_CUDA(cudaFuncSetAttribute(k_fix_medium, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFixMediumSmem));
+      attr = true;
+    }
+  }
+  k_fix_medium<<<device_sm_count(), kFixMedThreads, kFixMediumSmem, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaMemcpyAsync(host + 1, l.flags, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaMemcpyAsync(host + 2, l.fix.counts, 4 * sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaStreamSynchronize(s));
+  JFX_TRY(check_err_word((u32)host[0]));
+  const u32 ok = (u32)host[1];
+  const u32* cnts = (const u32*)(host + 2);
+  if (!ok || cnts[2]) {
+    // model not monotone, or a run the fix-up cannot take: plain radix sort
+    JFX_TRY(plain_sort_u64(keys, N, sorted_keys_out, (u32*)perm_out, b, c, s));
+    JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+    return check_err_word((u32)host[0]);
+  }
+  if (learned_used) *learned_used = 1;
+  return JFX_OK;
 }
 
 }  // extern "C"

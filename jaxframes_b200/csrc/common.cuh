@@ -287,7 +287,13 @@ struct Arena {
 };
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
-inline int bit_length(u64 v) { return v ? 64 - __builtin_clzll(v) : 0; }
+__host__ __device__ inline int bit_length(u64 v) {
+#ifdef __CUDA_ARCH__
+  return v ? 64 - __clzll((long long)v) : 0;
+#else
+  return v ? 64 - __builtin_clzll(v) : 0;
+#endif
+}
 
 // Number of SMs of the current device (cached per device).
 int device_sm_count();

@@ -1,0 +1,454 @@
+// learned.cuh -- learned-CDF partitioned sort of uint64 keys.  No counterpart
+// in the reference; its output is defined as the plain radix sort's.
+//
+// 1. A strided sample (1 key in 100) is sorted by the plain radix sort; the
+//    sample ranks are the labels.
+// 2. A two-level piecewise-linear model is fitted by least squares: a root
+//    linear model on model_feature(x) picks one of 4096 leaves; each leaf is a
+//    line rank ~ base + slope * (x - x0) clamped to the leaf's rank range
+//    (radix.cuh: model_pos).  Slopes are forced >= 0 and leaf ranges are
+//    disjoint and increasing, so the predicted position is monotone in x;
+//    k_leaf_finalize verifies it.
+// 3. Stable radix passes over the bits of the predicted position (not of x)
+//    move (key, row id) pairs: ceil(log2(n) / 11) passes instead of
+//    ceil(63 / 11).
+// 4. The position is monotone, so keys with different positions are already
+//    in order and only runs of equal position can hold inversions.
+//    k_fix_find lists the runs that hold one; k_fix_small (a warp per run)
+//    and k_fix_medium (a block radix sort per run) sort them by key -- equal
+//    keys keep row order because every pass is stable.  A run longer than
+//    kFixMaxRun, a full run list or a failed check make the caller fall back
+//    to the plain radix sort.  Either way the output equals the plain sort's.
+#pragma once
+
+#include "radix.cuh"
+
+namespace jfx {
+
+constexpr int kSampleStride = 100;
+
+__global__ void k_sample(const u64* keys, u64 stride, u64 s, u64* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (u64)gridDim.x * blockDim.x)
+    out[i] = keys[i * stride];
+}
+
+// Root fit, pass 1: acc[0] = sum of the feature over the sorted sample.
+__global__ void __launch_bounds__(256) k_root_sum(const u64* sx, u64 s, double* acc) {
+  double a = 0;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (u64)gridDim.x * blockDim.x)
+    a += model_feature(sx[i]);
+  for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&acc[0], a);
+}
+
+// Root fit, pass 2: centred covariance of (feature, rank) and feature variance.
+__global__ void __launch_bounds__(256) k_root_cov(const u64* sx, u64 s, double* acc) {
+  const double mf = acc[0] / (double)s, mr = 0.5 * (double)(s - 1);
+  double c = 0, v = 0;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (u64)gridDim.x * blockDim.x) {
+    const double df = model_feature(sx[i]) - mf;
+    c += df * ((double)i - mr);
+    v += df * df;
+  }
+  for (int o = 16; o; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[1], c);
+    atomicAdd(&acc[2], v);
+  }
+}
+
+// Root line: leaf coordinate = L/s * (mr + slope * (f - mf)).
+__global__ void k_root_solve(const double* acc, u64 s, ModelRef* m, Leaf* leaves) {
+  const double mf = acc[0] / (double)s, mr = 0.5 * (double)(s - 1);
+  double slope = acc[2] > 0 ? acc[1] / acc[2] : 0.0;
+  if (!(slope >= 0)) slope = 0;
+  const double k = (double)kLeaves / (double)s;
+  m->ra = slope * k;
+  m->rb = (mr - slope * mf) * k;
+  m->leaves = leaves;
+}
+
+// First and one-past-last sample index of every leaf (the sample is sorted
+// and the leaf index is monotone, so each leaf's points are contiguous).
+__global__ void k_leaf_bounds(const u64* sx, u64 s, const ModelRef* mp, u32* first, u32* last) {
+  const ModelRef m = *mp;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (u64)gridDim.x * blockDim.x) {
+    const int l = model_leaf(m, sx[i]);
+    if (i == 0 || model_leaf(m, sx[i - 1]) != l) first[l] = (u32)i;
+    if (i + 1 == s || model_leaf(m, sx[i + 1]) != l) last[l] = (u32)(i + 1);
+  }
+}
+
+// Least-squares line rank ~ base + slope * (x - x0) per leaf (a warp per leaf).
+__global__ void __launch_bounds__(256) k_leaf_fit(const u64* sx, const u32* first, const u32* last, double* fit) {
+  const int l = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (l >= kLeaves) return;
+  const u32 s0 = first[l];
+  if (s0 == 0xffffffffu) return;
+  const u32 e0 = last[l];
+  const u64 x0 = sx[s0];
+  const double cnt = (double)(e0 - s0);
+  double sd = 0;
+  for (u32 i = s0 + lane; i < e0; i += 32) sd += (double)(sx[i] - x0);
+  for (int o = 16; o; o >>= 1) sd += __shfl_xor_sync(0xffffffffu, sd, o);
+  const double md = sd / cnt, mr = 0.5 * ((double)s0 + (double)(e0 - 1));
+  double c = 0, v = 0;
+  for (u32 i = s0 + lane; i < e0; i += 32) {
+    const double dd = (double)(sx[i] - x0) - md;
+    c += dd * ((double)i - mr);
+    v += dd * dd;
+  }
+  for (int o = 16; o; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  if (lane == 0) {
+    double slope = v > 0 ? c / v : 0.0;
+    if (!(slope >= 0)) slope = 0;
+    fit[2 * l] = slope;
+    fit[2 * l + 1] = mr - slope * md;  // rank predicted at x0
+  }
+}
+
+// Leaf table in output positions.  An empty leaf collapses onto the start of
+// the next non-empty one.  ok[0] is cleared if the model is not monotone.
+__global__ void __launch_bounds__(1024) k_leaf_finalize(const u64* sx, u64 s, u64 n, const u32* first,
+                                                        const u32* last, const double* fit, Leaf* leaves,
+                                                        u32* ok) {
+  __shared__ u32 nf[kLeaves];
+  const double scale = (double)n / (double)s;
+  for (int l = threadIdx.x; l < kLeaves; l += 1024) nf[l] = first[l] == 0xffffffffu ? (u32)s : first[l];
+  __syncthreads();
+  for (int off = 1; off < kLeaves; off <<= 1) {  // suffix minimum
+    u32 tmp[kLeaves / 1024];
+#pragma unroll
+    for (int k = 0; k < kLeaves / 1024; ++k) {
+      const int l = threadIdx.x + k * 1024;
+      tmp[k] = l + off < kLeaves ? min(nf[l], nf[l + off]) : nf[l];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kLeaves / 1024; ++k) nf[threadIdx.x + k * 1024] = tmp[k];
+    __syncthreads();
+  }
+  for (int l = threadIdx.x; l < kLeaves; l += 1024) {
+    Leaf lf;
+    const bool empty = first[l] == 0xffffffffu;
+    const u32 s0 = empty ? nf[l] : first[l];
+    const u32 e0 = empty ? nf[l] : last[l];
+    lf.lo = (u32)fmin((double)n, floor((double)s0 * scale));
+    lf.hi = (u32)fmin((double)n, floor((double)e0 * scale));
+    if (lf.hi < lf.lo) lf.hi = lf.lo;
+    if (empty) {
+      lf.x0 = 0;
+      lf.slope = 0;
+      lf.base = (double)lf.lo;
+    } else {
+      lf.x0 = sx[s0];
+      lf.slope = fit[2 * l] * scale;
+      lf.base = fit[2 * l + 1] * scale;
+    }
+    if (!(lf.slope >= 0) || !(lf.base == lf.base)) atomicExch(ok, 0u);
+    leaves[l] = lf;
+  }
+  __syncthreads();
+  for (int l = threadIdx.x; l + 1 < kLeaves; l += 1024) {
+    if (leaves[l].hi > leaves[l + 1].lo || leaves[l].lo > leaves[l + 1].lo) atomicExch(ok, 0u);
+  }
+}
+
+// ------------------------------------------------------------------ fix-up ---
+constexpr int kFindTile = 2048, kFindThreads = 256;
+constexpr int kFixMaxRun = 6144;   // longest run the block sort takes
+constexpr int kFixSmall = 32;      // runs up to this length: one warp
+
+struct FixLists {
+  u32* small;       // [cap_small][2] (start, end)
+  u32* medium;      // [cap_medium][2]
+  u32* counts;      // [0] small, [1] medium, [2] overflow flag
+  u32* last_start;  // [tiles] last run start in the tile, or ~0
+  u32* carried_inv; // [tiles] first inversion of the run carried into the tile, or ~0
+  u32 cap_small, cap_medium;
+};
+
+__device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
+  const u64 len = e - s;
+  if (len > (u64)kFixMaxRun) {
+    atomicExch(&L.counts[2], 1u);
+    return;
+  }
+  if (len <= (u64)kFixSmall) {
+    const u32 r = atomicAdd(&L.counts[0], 1u);
+    if (r >= L.cap_small) { atomicExch(&L.counts[2], 1u); return; }
+    L.small[2 * r] = (u32)s;
+    L.small[2 * r + 1] = (u32)e;
+  } else {
+    const u32 r = atomicAdd(&L.counts[1], 1u);
+    if (r >= L.cap_medium) { atomicExch(&L.counts[2], 1u); return; }
+    L.medium[2 * r] = (u32)s;
+    L.medium[2 * r + 1] = (u32)e;
+  }
+}
+
+// Lists the runs of equal predicted position that start in this CTA's tile
+// and contain an inversion.
+__global__ void __launch_bounds__(kFindThreads) k_fix_find(const u64* keys, u64 n, const ModelRef* mp,
+                                                           FixLists L) {
+  __shared__ u64 sk[kFindTile + 1];
+  __shared__ u32 sp[kFindTile + 1];
+  __shared__ u32 fb[kFindTile / 32 + 2], ib[kFindTile / 32 + 2];
+  __shared__ int s_open;
+  const ModelRef m = *mp;
+  const u64 t0 = (u64)blockIdx.x * kFindTile;
+  const u64 t1 = min(n, t0 + kFindTile);
+  const u64 base = t0 ? t0 - 1 : 0;
+  const u32 len = (u32)(t1 - base);  // window: [base, t1)
+  for (u32 i = threadIdx.x; i < len; i += kFindThreads) {
+    const u64 k = keys[base + i];
+    sk[i] = k;
+    sp[i] = model_pos(m, k);
+  }
+  if (threadIdx.x == 0) s_open = -1;
+  __syncthreads();
+  // bit i of fb: window position i starts a run; of ib: it is an inversion
+  const int lane = threadIdx.x & 31;
+  for (u32 w0 = (threadIdx.x >> 5) * 32; w0 < len; w0 += kFindThreads) {
+    const u32 i = w0 + lane;
+    bool f = false, v = false;
+    if (i < len) {
+      if (base + i == 0) f = true;
+      else if (i > 0) {
+        f = sp[i] != sp[i - 1];
+        v = !f && sk[i - 1] > sk[i];
+      }
+    }
+    const u32 bf = __ballot_sync(0xffffffffu, f), bi = __ballot_sync(0xffffffffu, v);
+    if (lane == 0) {
+      fb[w0 >> 5] = bf;
+      ib[w0 >> 5] = bi;
+    }
+  }
+  __syncthreads();
+  const u32 off = t0 ? 1u : 0u;
+  const u32 nwords = (len + 31) >> 5;
+  if (threadIdx.x == 0) {
+    // tile summary: last run start, and the first inversion of the run that
+    // was carried in from earlier tiles (positions before the first start)
+    u32 first = len, lastp = 0xffffffffu;
+    for (u32 w = 0; w < nwords; ++w) {
+      u32 b = fb[w];
+      if (w == 0 && off) b &= ~1u;
+      if (b) {
+        if (first == len) first = (w << 5) + __ffs(b) - 1;
+        lastp = (w << 5) + 31 - __clz(b);
+      }
+    }
+    u32 cinv = 0xffffffffu;
+    for (u32 q = off; q < first && cinv == 0xffffffffu; ++q)
+      if ((ib[q >> 5] >> (q & 31)) & 1u) cinv = q;
+    L.last_start[blockIdx.x] = lastp == 0xffffffffu ? lastp : (u32)(base + lastp);
+    L.carried_inv[blockIdx.x] = cinv == 0xffffffffu ? cinv : (u32)(base + cinv);
+  }
+  for (u32 i = off + threadIdx.x; i < len; i += kFindThreads) {
+    if (!((fb[i >> 5] >> (i & 31)) & 1u)) continue;
+    // next run start after i inside the window
+    u32 e = len;
+    u32 w = i >> 5;
+    u32 bits = fb[w] & ~((2u << (i & 31)) - 1u);
+    if ((i & 31) == 31) bits = 0;
+    while (true) {
+      if (bits) {
+        e = (w << 5) + __ffs(bits) - 1;
+        break;
+      }
+      if (++w >= nwords) break;
+      bits = fb[w];
+    }
+    if (e > len) e = len;
+    if (e == len && t1 < n) {  // continues past the tile: finished by warp 0
+      s_open = (int)i;
+      continue;
+    }
+    bool inv = false;
+    for (u32 q = i + 1; q < e && !inv; ++q) inv = (ib[q >> 5] >> (q & 31)) & 1u;
+    if (inv) fix_record(L, base + i, base + e);
+  }
+  __syncthreads();
+  if (s_open < 0 || threadIdx.x >= 32) return;
+  // the last run of the tile: scan on past the tile, 32 keys at a time
+  const u32 i = (u32)s_open;
+  const u32 p0 = sp[i];
+  bool inv = false;
+  for (u32 q = i + 1; q < len; ++q) inv |= (ib[q >> 5] >> (q & 31)) & 1u;
+  u64 prev_key = sk[len - 1];
+  u64 pos = t1;
+  u64 e = n;
+  while (pos < n) {
+    const u64 q = pos + lane;
+    const bool in = q < n;
+    const u64 k = in ? keys[q] : 0;
+    const bool same = in && model_pos(m, k) == p0;
+    const u32 bs = __ballot_sync(0xffffffffu, same);
+    const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
+    const u64 km = lane == 0 ? prev_key : kp;
+    // positions of this chunk that still belong to the run: a prefix of lanes
+    const u32 run_lanes = ~bs ? (u32)(__ffs(~bs) - 1) : 32u;
+    const bool vi = (u32)lane < run_lanes && km > k;
+    inv |= __ballot_sync(0xffffffffu, vi) != 0;
+    if (run_lanes < 32) {
+      e = pos + run_lanes;
+      break;
+    }
+    prev_key = __shfl_sync(0xffffffffu, k, 31);
+    pos += 32;
+    if (pos - (base + i) > (u64)kFixMaxRun) {
+      e = pos;
+      break;
+    }
+  }
+  // a run longer than the window: an inversion seen here cannot be fixed
+  // (overflow); one past the window is caught by k_fix_check
+  if (lane == 0 && inv) fix_record(L, base + i, e);
+}
+
+// A run carried into a tile with an inversion the run's owner did not scan
+// (more than kFixMaxRun past the run start) means overflow.
+__global__ void k_fix_check(u64 tiles, FixLists L) {
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += (u64)gridDim.x * blockDim.x) {
+    const u32 inv = L.carried_inv[t];
+    if (inv == 0xffffffffu) continue;
+    u32 start = 0xffffffffu;
+    for (u64 k = 1; k <= t && k <= (u64)(kFixMaxRun / kFindTile + 2); ++k) {
+      start = L.last_start[t - k];
+      if (start != 0xffffffffu) break;
+    }
+    if (start == 0xffffffffu || (u64)inv - start >= (u64)kFixMaxRun) atomicExch(&L.counts[2], 1u);
+  }
+}
+
+// Sorts each short run by key with one warp (rank counting).
+__global__ void __launch_bounds__(256) k_fix_small(u64* keys, u32* vals, FixLists L) {
+  const u32 cnt = min(L.counts[0], L.cap_small);
+  const int lane = threadIdx.x & 31;
+  for (u64 r = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < cnt; r += ((u64)gridDim.x * blockDim.x) >> 5) {
+    const u32 s = L.small[2 * r], e = L.small[2 * r + 1];
+    const u32 m = e - s;
+    u64 k = 0;
+    u32 v = 0;
+    if ((u32)lane < m) {
+      k = keys[s + lane];
+      v = vals[s + lane];
+    }
+    u32 rank = 0;
+    for (u32 q = 0; q < m; ++q) {
+      const u64 kq = __shfl_sync(0xffffffffu, k, q);
+      rank += (kq < k) || (kq == k && q < (u32)lane);
+    }
+    __syncwarp();
+    if ((u32)lane < m) {
+      keys[s + rank] = k;
+      vals[s + rank] = v;
+    }
+  }
+}
+
+// Sorts each medium run with a block-wide stable LSD radix sort in shared
+// memory (8-bit digits of key - min over bit_length(max - min) bits).
+constexpr int kFixMedThreads = 256;
+__global__ void __launch_bounds__(kFixMedThreads) k_fix_medium(u64* keys, u32* vals, FixLists L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  u64* ka = (u64*)smem;                  // [kFixMaxRun]
+  u64* kb = ka + kFixMaxRun;             // [kFixMaxRun]
+  uint16_t* ia = (uint16_t*)(kb + kFixMaxRun);  // [kFixMaxRun] local indices
+  uint16_t* ib2 = ia + kFixMaxRun;
+  u32* sv = (u32*)(ib2 + kFixMaxRun);    // [kFixMaxRun] values
+  u32* wh = sv + kFixMaxRun;             // [8][256]
+  u32* tot = wh + 8 * 256;               // [256]
+  __shared__ u64 s_min, s_max;
+  __shared__ u32 scan_scratch[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32 cnt = min(L.counts[1], L.cap_medium);
+  for (u32 r = blockIdx.x; r < cnt; r += gridDim.x) {
+    const u32 s = L.medium[2 * r], e = L.medium[2 * r + 1];
+    const u32 m = e - s;
+    if (tid == 0) {
+      s_min = ~0ull;
+      s_max = 0;
+    }
+    __syncthreads();
+    u64 lmin = ~0ull, lmax = 0;
+    for (u32 j = tid; j < m; j += kFixMedThreads) {
+      const u64 k = keys[s + j];
+      ka[j] = k;
+      ia[j] = (uint16_t)j;
+      sv[j] = vals[s + j];
+      lmin = k < lmin ? k : lmin;
+      lmax = k > lmax ? k : lmax;
+    }
+    atomicMin(&s_min, lmin);
+    atomicMax(&s_max, lmax);
+    __syncthreads();
+    const u64 mn = s_min;
+    const int bits = bit_length(s_max - mn);
+    const u32 seg = (m + 7) / 8;  // warp w sorts positions [w*seg, (w+1)*seg) in order
+    u64 *src = ka, *dst = kb;
+    uint16_t *isrc = ia, *idst = ib2;
+    for (int sh = 0; sh < bits; sh += 8) {
+      for (int i = tid; i < 8 * 256; i += kFixMedThreads) wh[i] = 0;
+      __syncthreads();
+      const u32 w0 = warp * seg, w1 = min(m, w0 + seg);
+      for (u32 j = w0 + lane; j < w1; j += 32) atomicAdd(&wh[warp * 256 + (u32)(((src[j] - mn) >> sh) & 255u)], 1u);
+      __syncthreads();
+      for (int d = tid; d < 256; d += kFixMedThreads) {
+        u32 run = 0;
+        for (int w = 0; w < 8; ++w) {
+          const u32 c = wh[w * 256 + d];
+          wh[w * 256 + d] = run;
+          run += c;
+        }
+        tot[d] = run;
+      }
+      __syncthreads();
+      block_exclusive_scan<kFixMedThreads, 256>(tot, scan_scratch);
+      for (int d = tid; d < 256; d += kFixMedThreads)
+        for (int w = 0; w < 8; ++w) wh[w * 256 + d] += tot[d];
+      __syncthreads();
+      const u32 lt = lanemask_lt(), gt = lanemask_gt();
+      for (u32 j0 = w0; j0 < w1; j0 += 32) {
+        const u32 j = j0 + lane;
+        const bool in = j < w1;
+        const u32 d = in ? (u32)(((src[j] - mn) >> sh) & 255u) : 256u;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const u32 prior = in ? wh[warp * 256 + d] : 0u;
+        const u32 dst_i = prior + __popc(peers & lt);
+        __syncwarp();
+        if (in && !(peers & gt)) wh[warp * 256 + d] = prior + __popc(peers);
+        __syncwarp();
+        if (in) {
+          dst[dst_i] = src[j];
+          idst[dst_i] = isrc[j];
+        }
+      }
+      __syncthreads();
+      u64* t = src;
+      src = dst;
+      dst = t;
+      uint16_t* ti = isrc;
+      isrc = idst;
+      idst = ti;
+    }
+    for (u32 j = tid; j < m; j += kFixMedThreads) {
+      keys[s + j] = src[j];
+      vals[s + j] = sv[isrc[j]];
+    }
+    __syncthreads();
+  }
+}
+
+constexpr size_t kFixMediumSmem = (size_t)kFixMaxRun * (8 + 8 + 2 + 2 + 4) + (8 * 256 + 256) * 4;
+
+}  // namespace jfx

@@ -49,7 +49,49 @@ enum : int {
   KEY_HASH = 1,   // first pass hashes the key columns (hash_multi_columns)
   DIG_BITS = 0,   // digit = (key >> shift) & mask
   DIG_MOD = 1,    // digit = key % modulus (hash partition)
+  DIG_MODEL = 2,  // digit = (model position of key >> shift) & mask (learned sort)
 };
+
+// ---- learned-CDF model (fitted in learned.cuh), evaluated inside the passes
+constexpr int kLeaves = 4096;
+
+struct Leaf {
+  u64 x0;        // first sampled key of the leaf
+  double slope;  // positions per key unit (>= 0)
+  double base;   // predicted position at x0
+  u32 lo, hi;    // the leaf's position range [lo, hi)
+};
+
+struct ModelRef {
+  double ra, rb;       // leaf coordinate = ra * feature(x) + rb
+  const Leaf* leaves;  // [kLeaves]
+};
+
+// Monotone, log-like feature: the bit pattern of (double)x read as a number.
+__device__ __forceinline__ double model_feature(u64 x) {
+  return (double)__double_as_longlong((double)x);
+}
+
+__device__ __forceinline__ int model_leaf(const ModelRef& m, u64 x) {
+  const double lf = m.ra * model_feature(x) + m.rb;
+  if (!(lf > 0.0)) return 0;
+  if (lf >= (double)(kLeaves - 1)) return kLeaves - 1;
+  return (int)lf;
+}
+
+// Predicted output position of key x: monotone non-decreasing in x.
+__device__ __forceinline__ u32 model_pos(const ModelRef& m, u64 x) {
+  const Leaf* lp = m.leaves + model_leaf(m, x);
+  const u64 x0 = __ldg(&lp->x0);
+  const double slope = __ldg(&lp->slope), base = __ldg(&lp->base);
+  const u32 lo = __ldg(&lp->lo), hi = __ldg(&lp->hi);
+  const double d = x >= x0 ? (double)(x - x0) : -(double)(x0 - x);
+  const double p = base + slope * d;
+  const u32 top = hi > lo ? hi - 1 : lo;
+  if (!(p > (double)lo)) return lo;
+  if (p >= (double)top) return top;
+  return (u32)p;
+}
 
 struct PassArgs {
   const void* keys_in;   // K[n] (not read by the first pass)
@@ -67,6 +109,11 @@ struct PassArgs {
   int key_mode, digit_mode;
   u32 modulus;
   int reverse;           // write position n-1-p (descending radix sort)
+  void* raw_out;         // last pass: write the original integer key here instead of keys_out
+  int raw_dtype;
+  u32 raw_flags;
+  u64 raw_tmin;
+  const ModelRef* model; // DIG_MODEL: device-resident model
   PackDesc pack;
 };
 
@@ -112,8 +159,9 @@ __device__ __forceinline__ u32 hash_row(const PackDesc& pd, size_t row) {
 }
 
 template <typename K>
-__device__ __forceinline__ u32 digit_of(K key, int mode, int shift, u32 mask, u32 modulus) {
+__device__ __forceinline__ u32 digit_of(K key, int mode, int shift, u32 mask, u32 modulus, const ModelRef& m) {
   if (mode == DIG_MOD) return (u32)key % modulus;
+  if (mode == DIG_MODEL) return (model_pos(m, (u64)key) >> shift) & mask;
   return (u32)(key >> shift) & mask;
 }
 
@@ -255,6 +303,9 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   const u64 base = (u64)tile * TILE;
   const u32 tile_n = (u32)min((u64)TILE, a.n - base);
   const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
+  ModelRef model;
+  if (a.digit_mode == DIG_MODEL) model = *a.model;
+  else model.leaves = nullptr;
 
   K key[IPT];
   u32 val[IPT], dig[IPT];
@@ -272,7 +323,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
         key[i] = ((const K*)a.keys_in)[idx];
         val[i] = a.vals_in[idx];
       }
-      dig[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus);
+      dig[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
     }
   }
 
@@ -353,14 +404,15 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   K* kout = (K*)a.keys_out;
   for (u32 j = tid; j < tile_n; j += THREADS) {
     const K k = skeys[j];
-    const u32 d = digit_of<K>(k, a.digit_mode, a.shift, mask, a.modulus);
+    const u32 d = digit_of<K>(k, a.digit_mode, a.shift, mask, a.modulus, model);
     u64 g = (u64)(u32)(sbase[d] + j);
     if (g >= a.n) {  // only reachable if histogram and pass disagree
       atomicOr(a.err, DERR_BOUNDS);
       continue;
     }
     if (a.reverse) g = a.n - 1 - g;
-    kout[g] = k;
+    if (a.raw_out) store_raw(a.raw_out, a.raw_dtype, g, untransform_int(a.raw_dtype, a.raw_flags, (u64)k + a.raw_tmin));
+    else kout[g] = k;
     a.vals_out[g] = svals[j];
   }
   if (a.status_next)
@@ -378,6 +430,7 @@ struct HistArgs {
   u32 modulus;
   int shift[8];
   int width[8];
+  const ModelRef* model;
 };
 
 template <typename K, int RB>
@@ -390,13 +443,25 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
   u32 mask[8];
 #pragma unroll
   for (int p = 0; p < 8; ++p) mask[p] = a.width[p] >= 32 ? 0xffffffffu : ((1u << a.width[p]) - 1u);
+  ModelRef model;
+  if (a.digit_mode == DIG_MODEL) model = *a.model;
+  else model.leaves = nullptr;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < a.n; r += stride) {
     const K k = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, r) : pack_row<K>(a.pack, r);
+    if (a.digit_mode == DIG_MODEL) {
+      const u32 pos = model_pos(model, (u64)k);
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        if (p >= a.npass) break;
+        atomicAdd(&sh[p * RADIX + ((pos >> a.shift[p]) & mask[p])], 1u);
+      }
+      continue;
+    }
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
       if (p >= a.npass) break;
-      const u32 d = digit_of<K>(k, a.digit_mode, a.shift[p], mask[p], a.modulus);
+      const u32 d = digit_of<K>(k, a.digit_mode, a.shift[p], mask[p], a.modulus, model);
       atomicAdd(&sh[p * RADIX + d], 1u);
       if (p == 0 && a.targets) a.targets[r] = d;
     }
@@ -641,6 +706,13 @@ struct RadixRequest {
   bool key64 = false;        // packed key type
   void* keys_result = nullptr; // filled: where the sorted packed keys ended up
   int npass = 0;               // filled: passes run
+  // optional: the last pass writes the original integer key (single column)
+  // instead of the packed key
+  void* raw_out = nullptr;
+  int raw_dtype = 0;
+  u32 raw_flags = 0;
+  u64 raw_tmin = 0;
+  const ModelRef* model = nullptr;  // DIG_MODEL
 };
 
 template <typename K, int RB>
@@ -677,6 +749,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   h.key_mode = rq.key_mode;
   h.digit_mode = rq.digit_mode;
   h.modulus = rq.modulus;
+  h.model = rq.model;
   for (int p = 0; p < 8; ++p) {
     h.shift[p] = shift[p];
     h.width[p] = width[p];
@@ -717,7 +790,14 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     a.key_mode = rq.key_mode;
     a.digit_mode = rq.digit_mode;
     a.modulus = rq.modulus;
+    a.model = rq.model;
     a.reverse = last && rq.reverse;
+    if (last && rq.raw_out) {
+      a.raw_out = rq.raw_out;
+      a.raw_dtype = rq.raw_dtype;
+      a.raw_flags = rq.raw_flags;
+      a.raw_tmin = rq.raw_tmin;
+    }
     a.pack = rq.pack;
     if (p == 0) {
       JFX_TRY((launch_pass<K, RB, true>(a, n, s)));

@@ -29,7 +29,7 @@ __all__ = [
     "config", "ShardingSpec", "multi_column_lexsort", "hash_multi_columns", "combine_keys_for_sorting",
     "collective_hash_repartition", "compact_repartitioned_rows", "ParallelRadixSort", "SortBasedGroupBy",
     "ParallelSortMergeJoin", "parallel_sort", "groupby_aggregate", "groupby_aggregate_multi_column",
-    "sort_merge_join", "hash_partition",
+    "sort_merge_join", "hash_partition", "learned_sort",
 ]
 
 
@@ -530,6 +530,25 @@ class ParallelSortMergeJoin:
             dn = (right_value_dtypes or {}).get(name, str(t.dtype))
             vals[f"right_{name}"] = _gather_join_column(t, ri, dn, r_ok)
         return keys, vals
+
+
+def learned_sort(keys, mode: str = "auto"):
+    """Learned-CDF partitioned sort of uint64 keys (no reference counterpart):
+    ``(sorted_keys, perm int32, learned_used)``, identical to the plain radix
+    sort.  ``mode``: "auto" (learned with plain fallback) or "plain"."""
+    k = as_device(keys)
+    if k.dtype != torch.uint64:
+        raise TypeError(f"learned_sort takes uint64 keys, got {k.dtype}")
+    n = k.numel()
+    out = _empty(n, torch.uint64, k)
+    perm = _empty(n, torch.int32, k)
+    used = ctypes.c_int32(0)
+    if n:
+        L = _lib.lib()
+        ws = _lib.workspace(_lib.WS_LEARNED, n, device=k.device)
+        check(L.jfx_learned_sort(k.data_ptr(), n, out.data_ptr(), perm.data_ptr(), 0 if mode == "auto" else 1,
+                                 ctypes.byref(used), ws.data_ptr(), ws.numel(), _stream()))
+    return out, perm, bool(used.value)
 
 
 def _default_spec(sharding_spec):

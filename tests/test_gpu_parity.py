@@ -339,3 +339,48 @@ def test_hash_values_all_dtypes(P):
         np.testing.assert_array_equal(_np(P.hash_multi_columns([c])), O.hash_multi_columns([c]))
     np.testing.assert_array_equal(_np(P.hash_multi_columns(cols)), O.hash_multi_columns(cols))
     np.testing.assert_array_equal(_np(P.hash_multi_columns([cols[-1]])), O.hash_multi_columns([cols[-1]]))
+
+
+# ----------------------------------------------------------- learned sort ---
+def _c4_like(n):
+    import bench
+    return bench.c4_keys(nblocks=max(1, n // 4096))
+
+
+@pytest.mark.parametrize("dist", ["c4", "uniform", "sorted", "reversed", "equal", "few", "narrow"])
+def test_learned_sort_matches_plain_and_oracle(P, dist):
+    """The learned-CDF sort's output is the plain radix sort's, bit for bit."""
+    rng = np.random.default_rng(len(dist))
+    n = 1 << 21
+    if dist == "c4":
+        k = _c4_like(n)
+    elif dist == "uniform":
+        k = rng.integers(0, 2**64 - 1, n, dtype=np.uint64, endpoint=True)
+    elif dist == "sorted":
+        k = np.sort(rng.integers(0, 2**63, n, dtype=np.uint64))
+    elif dist == "reversed":
+        k = np.sort(rng.integers(0, 2**63, n, dtype=np.uint64))[::-1].copy()
+    elif dist == "equal":
+        k = np.full(n, 77, dtype=np.uint64)
+    elif dist == "few":
+        k = rng.integers(0, 50, n).astype(np.uint64) * np.uint64(1 << 40)
+    else:
+        k = rng.integers(1 << 50, (1 << 50) + 100_000, n).astype(np.uint64)
+    ep = np.argsort(k, kind="stable")
+    sk, perm, used = P.learned_sort(k, mode="auto")
+    np.testing.assert_array_equal(_np(perm), ep)
+    np.testing.assert_array_equal(_np(sk), k[ep])
+    sk2, perm2, used2 = P.learned_sort(k, mode="plain")
+    assert not used2
+    np.testing.assert_array_equal(_np(perm2), ep)
+    np.testing.assert_array_equal(_np(sk2), k[ep])
+    if dist in ("c4", "uniform", "sorted"):
+        assert used, "expected the learned path to be taken"
+
+
+def test_learned_sort_small_inputs_use_plain(P):
+    for n in (0, 1, 5, 1000):
+        k = np.random.default_rng(n).integers(0, 2**63, n, dtype=np.uint64)
+        sk, perm, used = P.learned_sort(k)
+        assert not used
+        np.testing.assert_array_equal(_np(perm), np.argsort(k, kind="stable"))
