@@ -180,6 +180,16 @@ int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out,
                      int mode, int32_t* learned_used, void* workspace, size_t workspace_bytes,
                      void* stream);
 
+/* Tuning of this thread's later calls (no counterpart in the reference): the
+ * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width)).
+ * jfx_set_tuning(NULL) restores the defaults.  The autotuner
+ * (jaxframes_b200/autotune.py) picks values per key dtype, size and skew. */
+typedef struct {
+  int32_t max_digit_bits;
+} jfx_tuning;
+int jfx_set_tuning(const jfx_tuning* t);
+int jfx_get_tuning(jfx_tuning* t);
+
 /* Measurement hooks.  No counterpart in the reference, which has no tracing.
  * jfx_launch_count: number of kernels this library has launched so far.
  * jfx_timing_enable(1) clears and starts CUDA-event timing of the radix pass

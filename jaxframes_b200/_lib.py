@@ -59,6 +59,10 @@ class AggColumn(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("max_digit_bits", ctypes.c_int32)]
+
+
 class JoinPlan(ctypes.Structure):
     _fields_ = [("opaque", ctypes.c_uint64 * 160)]
 
@@ -87,6 +91,8 @@ SIGNATURES = {
     "jfx_hash_columns": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P]),
     "jfx_hash_partition": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, _P, _P, _P, _P, _SIZE, _P]),
     "jfx_learned_sort": (_INT, [_P, _I64, _P, _P, _INT, ctypes.POINTER(ctypes.c_int32), _P, _SIZE, _P]),
+    "jfx_set_tuning": (_INT, [ctypes.POINTER(Tuning)]),
+    "jfx_get_tuning": (_INT, [ctypes.POINTER(Tuning)]),
     "jfx_launch_count": (ctypes.c_uint64, []),
     "jfx_timing_enable": (_INT, [_INT]),
     "jfx_timing_read": (_INT, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I64),

@@ -7,6 +7,7 @@ namespace jfx {
 thread_local std::string g_last_error;
 thread_local HostScratch g_host;
 std::atomic<unsigned long long> g_launches{0};
+thread_local Tuning g_tuning;
 Timing g_timing;
 
 int device_sm_count() {
@@ -129,6 +130,8 @@ struct JoinPlan {
   u32* foff;
   u32* fpart;
   u32* ftotal;
+  u64* win;
+  u64 win_cap;  // tiles the window buffer holds
   ColDesc lc[kMaxCols];
   ColDesc rc[kMaxCols];
 };
@@ -138,7 +141,7 @@ constexpr u64 kJoinMagic = 0x6a66786a6f696e32ull;
 struct JoinBuffers {
   void *skL, *skR;
   u32 *pL, *pR, *lo, *cnt, *lo2, *cnt2, *flag, *foff, *fpart, *ftotal;
-  u64 *off, *partial, *total;
+  u64 *off, *partial, *total, *win;
 };
 static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
   take_common(ar, c);
@@ -159,11 +162,12 @@ static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, Joi
   j.foff = ar.take<u32>(nmax ? nmax : 1);
   j.fpart = ar.take<u32>(scan_partials_count(nmax));
   j.ftotal = ar.take<u32>(4);
+  j.win = ar.take<u64>(2 * ((nmax + kJoinTile - 1) / kJoinTile + 1));
 }
 
 template <typename K>
 static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* lo, u32* cnt, const PackDesc& pd,
-                             cudaStream_t s) {
+                             u64* win, cudaStream_t s) {
   if (!na) return JFX_OK;
   if (!nb) {
     JFX_CUDA(cudaMemsetAsync(cnt, 0, na * sizeof(u32), s));
@@ -171,7 +175,8 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
     return JFX_OK;
   }
   const unsigned blocks = (unsigned)((na + kJoinTile - 1) / kJoinTile);
-  k_join_count<K><<<blocks, kJoinThreads, 0, s>>>((const K*)A, na, (const K*)B, nb, lo, cnt, pd), note_launch();
+  k_join_windows<K><<<(blocks + 255) / 256, 256, 0, s>>>((const K*)A, na, (const K*)B, nb, blocks, win), note_launch();
+  k_join_count<K><<<blocks, kJoinThreads, 0, s>>>((const K*)A, na, (const K*)B, nb, win, lo, cnt, pd), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }
@@ -256,6 +261,23 @@ extern "C" {
 const char* jfx_last_error(void) { return g_last_error.c_str(); }
 
 uint64_t jfx_launch_count(void) { return g_launches.load(); }
+
+int jfx_set_tuning(const jfx_tuning* t) {
+  if (!t) {
+    g_tuning = Tuning();
+    return JFX_OK;
+  }
+  if (t->max_digit_bits < 8 || t->max_digit_bits > 11)
+    return fail(JFX_ERR_ARG, "max_digit_bits must be in [8, 11], got %d", t->max_digit_bits);
+  g_tuning.max_digit_bits = t->max_digit_bits;
+  return JFX_OK;
+}
+
+int jfx_get_tuning(jfx_tuning* t) {
+  if (!t) return fail(JFX_ERR_ARG, "null pointer");
+  t->max_digit_bits = g_tuning.max_digit_bits;
+  return JFX_OK;
+}
 
 int jfx_timing_enable(int enable) {
   std::lock_guard<std::mutex> lk(g_timing.mu);
@@ -615,12 +637,12 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   const u64 na = swap ? nr : nl, nb = swap ? nl : nr;
   const void* A = swap ? j.skR : j.skL;
   const void* B = swap ? j.skL : j.skR;
-  if (key64) JFX_TRY(launch_join_count<u64>(A, na, B, nb, j.lo, j.cnt, pl, s));
-  else JFX_TRY(launch_join_count<u32>(A, na, B, nb, j.lo, j.cnt, pl, s));
+  if (key64) JFX_TRY(launch_join_count<u64>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s));
+  else JFX_TRY(launch_join_count<u32>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s));
   const bool rev = how == JFX_JOIN_OUTER;
   if (rev) {
-    if (key64) JFX_TRY(launch_join_count<u64>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, s));
-    else JFX_TRY(launch_join_count<u32>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, s));
+    if (key64) JFX_TRY(launch_join_count<u64>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, j.win, s));
+    else JFX_TRY(launch_join_count<u32>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, j.win, s));
   }
   host[1] = 0;
   if (na && nb) {
@@ -655,6 +677,8 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   jp->flag = j.flag;
   jp->foff = j.foff;
   jp->fpart = j.fpart;
+  jp->win = j.win;
+  jp->win_cap = (std::max(jp->nl, jp->nr) + kJoinTile - 1) / kJoinTile + 1;
   jp->ftotal = j.ftotal;
   for (int k = 0; k < ncols; ++k) {
     jp->lc[k] = pl.c[k];
@@ -687,11 +711,16 @@ int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* r
   int32_t* a_out = swap ? right_idx_out : left_idx_out;
   int32_t* b_out = swap ? left_idx_out : right_idx_out;
   if (jp->how == JFX_JOIN_INNER || jp->how == JFX_JOIN_OUTER) {
-    const unsigned blocks = (unsigned)((jp->m + kJoinTile - 1) / kJoinTile);
-    if (jp->key64)
-      k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko), note_launch();
-    else
-      k_join_expand_inner<u32><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko), note_launch();
+    // output tiles in chunks of the window buffer's capacity
+    const u64 tiles = (jp->m + kJoinTile - 1) / kJoinTile;
+    for (u64 t0 = 0; t0 < tiles; t0 += jp->win_cap) {
+      const unsigned blocks = (unsigned)std::min<u64>(jp->win_cap, tiles - t0);
+      k_expand_windows<<<(blocks + 255) / 256, 256, 0, s>>>(jp->off, na, jp->m, t0, blocks, jp->win), note_launch();
+      if (jp->key64)
+        k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko, t0), note_launch();
+      else
+        k_join_expand_inner<u32><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko, t0), note_launch();
+    }
   } else {
     const int g = grid_for(na, 256);
     if (jp->key64)

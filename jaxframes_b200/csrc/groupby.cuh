@@ -19,7 +19,7 @@
 namespace jfx {
 
 constexpr int kMaxVals = 16;
-constexpr int kGroupIPT = 16;
+constexpr int kGroupIPT = 8;
 constexpr u32 kEmptySlot = 0xffffffffu;
 
 enum : int { VK_F = 0, VK_I = 1, VK_U = 2 };
@@ -147,6 +147,29 @@ __device__ __forceinline__ Agg<KIND> agg_combine(const Agg<KIND>& a, const Agg<K
     r.mx = b.mx > a.mx ? b.mx : a.mx;
   }
   return r;
+}
+
+// The row's value as the 64-bit word the partial state holds.
+template <int KIND>
+__device__ __forceinline__ u64 value_word(const ValDesc& v, u64 row) {
+  if (KIND == VK_F) {
+    const double x = v.dtype == JFX_F32 ? (double)__ldg((const float*)v.ptr + row) : __ldg((const double*)v.ptr + row);
+    return __double_as_longlong(x);
+  }
+  if (KIND == VK_I) {
+    switch (v.dtype) {
+      case JFX_I8: return (u64)(long long)((const signed char*)v.ptr)[row];
+      case JFX_I16: return (u64)(long long)((const short*)v.ptr)[row];
+      case JFX_I32: return (u64)(long long)__ldg((const int*)v.ptr + row);
+      default: return (u64)__ldg((const long long*)v.ptr + row);
+    }
+  }
+  switch (v.dtype) {
+    case JFX_U8: case JFX_BOOL: return ((const unsigned char*)v.ptr)[row];
+    case JFX_U16: return ((const unsigned short*)v.ptr)[row];
+    case JFX_U32: return __ldg((const unsigned*)v.ptr + row);
+    default: return __ldg((const u64*)v.ptr + row);
+  }
 }
 
 template <int KIND>
@@ -299,6 +322,13 @@ __device__ __forceinline__ void reduce_column(const GroupArgs& a, int c, const u
   Agg<KIND> open = agg_identity<KIND>();
   bool open_valid = false, open_started = false;
   u32 open_gid = 0, gcount = 0;
+  // issue every gather of the warp's rows before the scan (memory-level parallelism)
+  u64 word[kGroupIPT];
+#pragma unroll
+  for (int s = 0; s < kGroupIPT; ++s) {
+    const u64 row = wbeg + (u64)s * 32 + lane;
+    word[s] = (need_vals && row < wend) ? value_word<KIND>(v, pr[s]) : 0ull;
+  }
 #pragma unroll
   for (int s = 0; s < kGroupIPT; ++s) {
     const u64 step0 = wbeg + (u64)s * 32;
@@ -308,8 +338,8 @@ __device__ __forceinline__ void reduce_column(const GroupArgs& a, int c, const u
     const u32 f = fm[s];
     Agg<KIND> st = agg_identity<KIND>();
     if (valid) {
-      if (need_vals) st = agg_of<KIND>(v, pr[s]);
-      else st.cnt = 1;
+      st.cnt = 1;
+      if (need_vals) st.sum = st.mn = st.mx = word[s];
     }
     const u32 hb = f & le;
     const int h = hb ? 31 - __clz(hb) : -1;
@@ -356,7 +386,7 @@ __device__ __forceinline__ void reduce_column(const GroupArgs& a, int c, const u
 }
 
 template <typename K>
-__global__ void __launch_bounds__(256) k_group_reduce(GroupArgs a, u64 nwarps) {
+__global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps) {
   const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nwarps) return;

@@ -39,20 +39,28 @@ __device__ __forceinline__ u64 upper_bound_g(const K* a, u64 lo, u64 hi, K x) {
 
 // For each sorted A row: lo = first B position with key >= A[i], cnt = number
 // of B keys equal to A[i] (0 for a NaN key, which equals nothing).
+// Window of B that the A tile of each count CTA can reach: [lower_bound of
+// its first key, upper_bound of its last key).  One thread per tile, all
+// searches in parallel (a CTA would otherwise start with a serial search).
+template <typename K>
+__global__ void k_join_windows(const K* A, u64 na, const K* B, u64 nb, u64 tiles, u64* win) {
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += (u64)gridDim.x * blockDim.x) {
+    const u64 a0 = t * kJoinTile, a1 = min(na, a0 + kJoinTile);
+    const u64 lo = lower_bound_g<K>(B, 0, nb, A[a0]);
+    win[2 * t] = lo;
+    win[2 * t + 1] = upper_bound_g<K>(B, lo, nb, A[a1 - 1]);
+  }
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kJoinThreads) k_join_count(const K* A, u64 na, const K* B, u64 nb,
-                                                            u32* lo_out, u32* cnt_out, PackDesc pd) {
+                                                            const u64* windows, u32* lo_out, u32* cnt_out,
+                                                            PackDesc pd) {
   constexpr int CAP = (32 * 1024) / sizeof(K);
   __shared__ K win[CAP];
-  __shared__ u64 wlo_s, whi_s;
   const u64 a0 = (u64)blockIdx.x * kJoinTile;
   const u64 a1 = min(na, a0 + kJoinTile);
-  if (threadIdx.x == 0) {
-    wlo_s = lower_bound_g<K>(B, 0, nb, A[a0]);
-    whi_s = upper_bound_g<K>(B, wlo_s, nb, A[a1 - 1]);
-  }
-  __syncthreads();
-  const u64 wlo = wlo_s, whi = whi_s, wn = whi - wlo;
+  const u64 wlo = windows[2 * blockIdx.x], whi = windows[2 * blockIdx.x + 1], wn = whi - wlo;
   const bool in_smem = wn <= (u64)CAP;
   if (in_smem)
     for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = B[wlo + i];
@@ -99,23 +107,28 @@ __device__ __forceinline__ void write_join_key(const JoinKeyOut& ko, u64 o, K pa
 }
 
 // Inner join: output o belongs to the sorted A row i with off[i] <= o < off[i+1].
+// Rows of A used by each expand CTA's output tile: [row of its first output,
+// one past the row of its last output).
+__global__ void k_expand_windows(const u64* off, u64 na, u64 m, u64 tile0, u64 tiles, u64* win) {
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += (u64)gridDim.x * blockDim.x) {
+    const u64 o0 = (tile0 + t) * kJoinTile, o1 = min(m, o0 + kJoinTile);
+    const u64 i0 = upper_bound_g<u64>(off, 0, na, o0) - 1;
+    win[2 * t] = i0;
+    win[2 * t + 1] = upper_bound_g<u64>(off, i0, na, o1 - 1);
+  }
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kJoinThreads) k_join_expand_inner(const u64* off, u64 na, u64 m,
-                                                                   const u32* lo, const u32* pA,
-                                                                   const u32* pB, const K* skA,
+                                                                   const u64* windows, const u32* lo,
+                                                                   const u32* pA, const u32* pB, const K* skA,
                                                                    int32_t* a_out, int32_t* b_out,
-                                                                   JoinKeyOut ko) {
+                                                                   JoinKeyOut ko, u64 tile0) {
   constexpr int CAP = 4096;
   __shared__ u64 win[CAP];
-  __shared__ u64 i0_s, i1_s;
-  const u64 o0 = (u64)blockIdx.x * kJoinTile;
+  const u64 o0 = (tile0 + blockIdx.x) * kJoinTile;
   const u64 o1 = min(m, o0 + kJoinTile);
-  if (threadIdx.x == 0) {
-    i0_s = upper_bound_g<u64>(off, 0, na, o0) - 1;
-    i1_s = upper_bound_g<u64>(off, i0_s, na, o1 - 1);  // one past the last row used
-  }
-  __syncthreads();
-  const u64 i0 = i0_s, i1 = i1_s, wn = i1 - i0;
+  const u64 i0 = windows[2 * blockIdx.x], i1 = windows[2 * blockIdx.x + 1], wn = i1 - i0;
   const bool in_smem = wn <= (u64)CAP;
   if (in_smem)
     for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = off[i0 + i];

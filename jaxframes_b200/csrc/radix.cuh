@@ -28,7 +28,7 @@ constexpr u32 ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_ERR = 3u << 30, ST_CNT = 
 
 template <int RB>
 struct RadixCfg {
-  static constexpr int THREADS = RB >= 11 ? 512 : 256;
+  static constexpr int THREADS = 256;
   static constexpr int IPT = 16;
 };
 
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   }
 
   // Resolve each digit's prefix over the earlier tiles and publish it.
-  constexpr int W = (RADIX / THREADS) >= 4 ? 8 : 16;
+  constexpr int W = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sbase[d];
     u32 excl = 0;
@@ -541,6 +541,12 @@ __global__ void k_fill_keys(K* out, u64 n) {
 }
 
 // ----------------------------------------------------------- host driver ---
+// Thread-local tuning (jfx_set_tuning): widest radix digit of a pass.
+struct Tuning {
+  int max_digit_bits = 11;
+};
+extern thread_local Tuning g_tuning;
+
 // Pinned host scratch for the few words an entry point reads back.
 struct HostScratch {
   u64* p = nullptr;
@@ -697,7 +703,7 @@ struct RadixRequest {
   int digit_mode = DIG_BITS;
   u32 modulus = 0;
   int total_bits = 0;        // packed key width (DIG_BITS)
-  int max_digit_bits = 11;   // widest digit allowed
+  int max_digit_bits = g_tuning.max_digit_bits;  // widest digit allowed
   bool reverse = false;      // descending: write n-1-p in the last pass
   const u32* gather_idx = nullptr;
   u32* targets = nullptr;    // hash partition: digit of each row (row order)

@@ -121,10 +121,12 @@ def _radix_sort_perm(keys: torch.Tensor, ascending: bool, want_keys: bool):
     perm = _empty(n, torch.int32, keys)
     sk = _empty(n, keys.dtype, keys) if want_keys else None
     if n:
+        from .autotune import applied
         ws = _lib.workspace(_lib.WS_SORT, n, device=keys.device)
         col = _lib.column(keys)
-        check(L.jfx_sort(ctypes.byref(col), n, 1 if ascending else 0, perm.data_ptr(),
-                         sk.data_ptr() if sk is not None else None, ws.data_ptr(), ws.numel(), _stream()))
+        with applied("sort", keys):
+            check(L.jfx_sort(ctypes.byref(col), n, 1 if ascending else 0, perm.data_ptr(),
+                             sk.data_ptr() if sk is not None else None, ws.data_ptr(), ws.numel(), _stream()))
     return perm, sk
 
 
