@@ -398,7 +398,7 @@ def run_secondary(args):
                 out = fn()
             b2.record()
             torch.cuda.synchronize()
-            res[mode] = {"ms": a.elapsed_time(b2) / args.steps, "learned_used": bool(out[2])}
+            res[mode] = {"ms": a.elapsed_time(b2) / args.steps, "learned_used": int(out[2])}
         same = bool(torch.equal(P.learned_sort(keys, mode="plain")[1], P.learned_sort(keys, mode="learned")[1]))
         print(json.dumps({"workload": "learned", "rows": n, **res, "identical_perm": same,
                           "speedup": res["plain"]["ms"] / res["learned"]["ms"]}), flush=True)

@@ -83,6 +83,7 @@ typedef struct {
 #define JFX_WS_JOIN 3      /* n1 = left rows, n2 = right rows */
 #define JFX_WS_PARTITION 4 /* n1 = rows, n2 = partitions */
 #define JFX_WS_LEARNED 5   /* n1 = rows (uint64 keys) */
+#define JFX_WS_BATCH 6     /* n1 = total rows, n2 = queries */
 
 const char* jfx_last_error(void);
 int jfx_version(void);
@@ -175,10 +176,38 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
  * sorted in a fix-up.  mode 0: learned, with the plain sort as fallback when
  * the model fails its monotonicity check or a run overflows the fix-up;
  * mode 1: plain radix sort only.  *learned_used (nullable) is 1 when the
- * learned path produced the result. */
+ * learned path produced the result, 0 when the plain sort was asked for or
+ * the input is small, and -1 / -2 / -3 when the learned path fell back
+ * (model check failed / a run of equal prediction too long / run list full). */
 int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out, int32_t* perm_out,
                      int mode, int32_t* learned_used, void* workspace, size_t workspace_bytes,
                      void* stream);
+
+/* Many independent queries in one launch sequence (no host synchronisation,
+ * so it can be captured in one CUDA graph).  Query q owns rows
+ * [query_offsets[q], query_offsets[q+1]) of keys/values (device int64[nq+1];
+ * n = query_offsets[nq], given by the host).  Per query it computes the
+ * one-device body of collective_hash_repartition with num_partitions
+ * partitions (parallel_algorithms.py:163-182, :213-214: partition
+ * fmix32(key) % P, stable) and SortBasedGroupBy.groupby_aggregate sum and
+ * count of the values (:733-803; count in the value dtype):
+ *   part_keys_out / part_values_out [n]: rows in partition order per query;
+ *   part_offsets_out [nq * (P+1)]: absolute row offsets of each partition;
+ *   group_keys_out / group_sums_out / group_counts_out [capacity n]: groups
+ *   of query q at [group_offsets_out[q], group_offsets_out[q+1]), keys
+ *   ascending.
+ * Keys must lie in [0, 2^key_bits); jfx_batch_status reports a violation.
+ * ceil(log2(nq)) + key_bits must not exceed 32. */
+int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const int64_t* query_offsets,
+                                int nq, int64_t n, int num_partitions, int key_bits,
+                                int32_t* part_keys_out, float* part_values_out,
+                                int64_t* part_offsets_out, int32_t* group_keys_out,
+                                float* group_sums_out, float* group_counts_out,
+                                int64_t* group_offsets_out, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
+/* Status of the batched call that last used this workspace (synchronises). */
+int jfx_batch_status(void* workspace, size_t workspace_bytes, void* stream);
 
 /* Tuning of this thread's later calls (no counterpart in the reference): the
  * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width)).

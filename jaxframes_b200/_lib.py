@@ -33,7 +33,7 @@ COL_DESC = 1
 AGG_SUM, AGG_MEAN, AGG_COUNT, AGG_MIN, AGG_MAX = 1, 2, 4, 8, 16
 AGG_BITS = {"sum": AGG_SUM, "mean": AGG_MEAN, "count": AGG_COUNT, "min": AGG_MIN, "max": AGG_MAX}
 JOIN_KINDS = {"inner": 0, "left": 1, "right": 2, "outer": 3}
-WS_SORT, WS_GROUPBY, WS_JOIN, WS_PARTITION, WS_LEARNED = 1, 2, 3, 4, 5
+WS_SORT, WS_GROUPBY, WS_JOIN, WS_PARTITION, WS_LEARNED, WS_BATCH = 1, 2, 3, 4, 5, 6
 
 
 class JfxUnavailable(RuntimeError):
@@ -91,6 +91,9 @@ SIGNATURES = {
     "jfx_hash_columns": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P]),
     "jfx_hash_partition": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, _P, _P, _P, _P, _SIZE, _P]),
     "jfx_learned_sort": (_INT, [_P, _I64, _P, _P, _INT, ctypes.POINTER(ctypes.c_int32), _P, _SIZE, _P]),
+    "jfx_batch_partition_groupby": (_INT, [_P, _P, _P, _INT, _I64, _INT, _INT, _P, _P, _P, _P, _P, _P, _P, _P,
+                                           _SIZE, _P]),
+    "jfx_batch_status": (_INT, [_P, _SIZE, _P]),
     "jfx_set_tuning": (_INT, [ctypes.POINTER(Tuning)]),
     "jfx_get_tuning": (_INT, [ctypes.POINTER(Tuning)]),
     "jfx_launch_count": (ctypes.c_uint64, []),

@@ -1,6 +1,7 @@
 // api.cu -- extern "C" entry points of libjfx (declared in include/jfx.h).
 #include "join.cuh"
 #include "learned.cuh"
+#include "batch.cuh"
 
 namespace jfx {
 
@@ -243,6 +244,61 @@ static int plain_sort_u64(const u64* keys, u64 n, u64* sorted_out, u32* perm_out
   return JFX_OK;
 }
 
+// ------------------------------------------------------------------ batch ---
+struct BatchBuffers {
+  u64* row_base;
+  u32* tile_cnt;
+  u32* tile_base;
+  u32* total_tiles;
+  u32* scan_part;
+  u32* tile_seg;
+  u32* hist;
+  u32* base;
+  u32* counters;
+  u32* status[2];
+  u32* keys[2];
+  u32* vals[2];
+  u32* sk;
+  u32* sv;
+  u32* group_q;
+  GroupBuffers g;
+  u64 max_tiles;
+};
+constexpr int kBatchRB = 10;  // digit width of the batched passes (RADIX 1024)
+
+static void carve_batch(Arena& ar, u64 n, u64 nq, Common& c, BatchBuffers& b) {
+  take_common(ar, c);
+  const u64 nn = n ? n : 1;
+  b.max_tiles = n / kBatchTile + nq + 1;
+  b.row_base = ar.take<u64>(nq + 2);
+  b.tile_cnt = ar.take<u32>(nq + 2);
+  b.tile_base = ar.take<u32>(nq + 2);
+  b.total_tiles = ar.take<u32>(4);
+  b.scan_part = ar.take<u32>(scan_partials_count(nq + 1));
+  b.tile_seg = ar.take<u32>(b.max_tiles);
+  b.hist = ar.take<u32>((nq + 1) * 4 * (1u << kBatchRB));
+  b.base = ar.take<u32>((nq + 1) * 4 * (1u << kBatchRB));
+  b.counters = ar.take<u32>(64);
+  b.status[0] = ar.take<u32>(b.max_tiles * (1u << kBatchRB));
+  b.status[1] = ar.take<u32>(b.max_tiles * (1u << kBatchRB));
+  b.keys[0] = ar.take<u32>(nn);
+  b.keys[1] = ar.take<u32>(nn);
+  b.vals[0] = ar.take<u32>(nn);
+  b.vals[1] = ar.take<u32>(nn);
+  b.sk = ar.take<u32>(nn);
+  b.sv = ar.take<u32>(nn);
+  b.group_q = ar.take<u32>(nn);
+  GroupBuffers& g = b.g;
+  g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
+  g.warp_count = ar.take<u32>(g.nwarps + 1);
+  g.warp_base = ar.take<u32>(g.nwarps + 1);
+  g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
+  g.total = ar.take<u32>(4);
+  g.slot_gid = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_started = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_state = ar.take<u64>(4 * (2 * g.nwarps + 1));
+}
+
 // -------------------------------------------------------------- partition ---
 static void carve_partition(Arena& ar, u64 n, Common& c, SortBuffers& b) { carve_sort(ar, n, c, b); }
 
@@ -335,6 +391,11 @@ size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2) {
     case JFX_WS_LEARNED: {
       LearnedBuffers l;
       carve_learned(ar, a, c, b, l);
+      break;
+    }
+    case JFX_WS_BATCH: {
+      BatchBuffers bb;
+      carve_batch(ar, a, bn, c, bb);
       break;
     }
     default:
@@ -918,7 +979,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   }
   // 4. fix-up of runs of equal predicted position
   JFX_CUDA(cudaMemsetAsync(l.fix.counts, 0, 8 * sizeof(u32), s));
-  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, N, l.model, l.fix), note_launch();
+  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, N, l.model, l.fix), note_launch();
   k_fix_check<<<grid_for(l.tiles, 256), 256, 0, s>>>(l.tiles, l.fix), note_launch();
   k_fix_small<<<device_sm_count() * 8, 256, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
   {
@@ -938,13 +999,206 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   const u32 ok = (u32)host[1];
   const u32* cnts = (const u32*)(host + 2);
   if (!ok || cnts[2]) {
-    // model not monotone, or a run the fix-up cannot take: plain radix sort
+    // model not monotone, or a run the fix-up cannot take: plain radix sort.
+    // *learned_used reports why: -1 model check, -2 run too long, -3 list full
+    const int why = !ok ? -1 : (cnts[2] & FIX_LONG_RUN) ? -2 : -3;
     JFX_TRY(plain_sort_u64(keys, N, sorted_keys_out, (u32*)perm_out, b, c, s));
     JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+    if (learned_used) *learned_used = why;
     return check_err_word((u32)host[0]);
   }
   if (learned_used) *learned_used = 1;
   return JFX_OK;
+}
+
+int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const int64_t* query_offsets, int nq,
+                                int64_t n, int num_partitions, int key_bits, int32_t* part_keys_out,
+                                float* part_values_out, int64_t* part_offsets_out, int32_t* group_keys_out,
+                                float* group_sums_out, float* group_counts_out, int64_t* group_offsets_out,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+  JFX_TRY(check_n(n));
+  if (nq < 1) return fail(JFX_ERR_ARG, "need at least one query");
+  if (num_partitions < 1 || num_partitions > 256) return fail(JFX_ERR_ARG, "num_partitions must be in [1, 256]");
+  if (key_bits < 1 || key_bits > 30) return fail(JFX_ERR_ARG, "key_bits must be in [1, 30]");
+  const int qbits = std::max(1, bit_length((u64)(nq - 1)));
+  if (qbits + key_bits > 32)
+    return fail(JFX_ERR_CAPACITY, "query id (%d bits) and key (%d bits) exceed 32 bits", qbits, key_bits);
+  if (!keys || !values || !query_offsets || !part_keys_out || !part_values_out || !part_offsets_out ||
+      !group_keys_out || !group_sums_out || !group_counts_out || !group_offsets_out)
+    return fail(JFX_ERR_ARG, "null pointer");
+  cudaStream_t s = as_stream(stream);
+  Arena ar(workspace, workspace_bytes);
+  Common c;
+  BatchBuffers bb;
+  carve_batch(ar, (u64)n, (u64)nq, c, bb);
+  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  constexpr int RB = kBatchRB, RADIX = 1 << RB;
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  // segment tables
+  const int gq = grid_for((u64)nq + 1, 256);
+  k_seg_setup<<<gq, 256, 0, s>>>(query_offsets, (u32)nq, bb.row_base, bb.tile_cnt, c.err), note_launch();
+  JFX_TRY(device_exclusive_scan<u32>(bb.tile_cnt, (u64)nq, bb.tile_base, bb.total_tiles, bb.scan_part, s));
+  JFX_CUDA(cudaMemcpyAsync(bb.tile_base + nq, bb.total_tiles, sizeof(u32), cudaMemcpyDeviceToDevice, s));
+  k_seg_tile_map<<<gq, 256, 0, s>>>(bb.tile_base, bb.tile_cnt, (u32)nq, bb.tile_seg), note_launch();
+  // histograms of the partition digit and the key digits, per query
+  const int npk = ceil_div(key_bits, RB);
+  const int npass = 1 + npk;
+  int shift[8] = {0}, width[8] = {0};
+  width[0] = 8;
+  {
+    const int bw = key_bits / npk, rem = key_bits % npk;
+    int at = 0;
+    for (int p = 1; p <= npk; ++p) {
+      width[p] = bw + (p - 1 < rem ? 1 : 0);
+      shift[p] = at;
+      at += width[p];
+    }
+  }
+  JFX_CUDA(cudaMemsetAsync(bb.hist, 0, (size_t)nq * npass * RADIX * sizeof(u32), s));
+  JFX_CUDA(cudaMemsetAsync(bb.counters, 0, 64 * sizeof(u32), s));
+  {
+    SegHistArgs h;
+    memset(&h, 0, sizeof h);
+    h.keys = keys;
+    h.row_base = bb.row_base;
+    h.tile_base = bb.tile_base;
+    h.tile_seg = bb.tile_seg;
+    h.total_tiles = bb.total_tiles;
+    h.hist = bb.hist;
+    h.err = c.err;
+    h.npass = npass;
+    h.modulus = (u32)num_partitions;
+    h.key_bits = key_bits;
+    for (int p = 0; p < 8; ++p) {
+      h.shift[p] = shift[p];
+      h.width[p] = width[p];
+    }
+    static bool attr = false;
+    if (!attr) {
+      JFX_CUDA(cudaFuncSetAttribute(k_hist_seg<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * RADIX * 4));
+      attr = true;
+    }
+    k_hist_seg<RB><<<device_sm_count() * 4, 256, npass * RADIX * sizeof(u32), s>>>(h), note_launch();
+  }
+  k_hist_scan<RB><<<(unsigned)(nq * npass), 1024, 0, s>>>(bb.hist, bb.base), note_launch();
+  JFX_CUDA(cudaMemsetAsync(bb.status[0], 0, bb.max_tiles * RADIX * sizeof(u32), s));
+  JFX_CUDA(cudaGetLastError());
+  // pass 0: stable partition by fmix32(key) % P, moving (key, value)
+  PassArgs a;
+  memset(&a, 0, sizeof a);
+  a.n = (u64)n;
+  a.err = c.err;
+  a.segmented = 1;
+  a.seg.row_base = bb.row_base;
+  a.seg.tile_base = bb.tile_base;
+  a.seg.tile_seg = bb.tile_seg;
+  a.seg.nseg = (u32)nq;
+  a.seg.total_tiles = bb.total_tiles;
+  a.seg.npass_stride = npass;
+  a.bin_base = bb.base;
+  {
+    jfx_column col{keys, JFX_I32, 0u};
+    JFX_TRY(build_pack(&col, 1, 0u, false, a.pack));
+    a.pack.c[0].bits = 32;
+  }
+  a.key_mode = KEY_PACK;
+  a.digit_mode = DIG_HASHMOD;
+  a.modulus = (u32)num_partitions;
+  a.width = RB;
+  a.vals_first = (const u32*)values;
+  a.raw_out = part_keys_out;
+  a.raw_dtype = JFX_I32;
+  a.keys_out = bb.keys[0];
+  a.vals_out = (u32*)part_values_out;
+  a.status = bb.status[0];
+  a.status_next = bb.status[1];
+  a.tile_counter = bb.counters;
+  a.seg.pass_index = 0;
+  JFX_TRY((launch_pass<u32, RB, true>(a, (u64)n, s, bb.max_tiles)));
+  {
+    const u64 tot = (u64)nq * (num_partitions + 1);
+    k_part_offsets<<<grid_for(tot, 256), 256, 0, s>>>(bb.row_base, bb.base, (u32)nq, npass, RADIX,
+                                                     (u32)num_partitions, part_offsets_out), note_launch();
+  }
+  // key passes over the partitioned rows, values carried
+  const u32* kin = (const u32*)part_keys_out;
+  const u32* vin = (const u32*)part_values_out;
+  for (int p = 1; p <= npk; ++p) {
+    const bool last = p == npk;
+    PassArgs b = a;
+    b.vals_first = nullptr;
+    b.raw_out = nullptr;
+    b.digit_mode = DIG_BITS;
+    b.shift = shift[p];
+    b.width = width[p];
+    b.keys_in = kin;
+    b.vals_in = vin;
+    b.keys_out = last ? bb.sk : bb.keys[p & 1];
+    b.vals_out = last ? bb.sv : bb.vals[p & 1];
+    b.status = bb.status[p & 1];
+    b.status_next = last ? nullptr : bb.status[(p + 1) & 1];
+    b.tile_counter = bb.counters + p;
+    b.seg.pass_index = p;
+    b.seg.key_shift_q = last ? key_bits : 0;
+    JFX_TRY((launch_pass<u32, RB, false>(b, (u64)n, s, bb.max_tiles)));
+    kin = (const u32*)b.keys_out;
+    vin = b.vals_out;
+  }
+  // groupby sum and count over the whole batch on (query, key) composite keys
+  GroupArgs ga;
+  memset(&ga, 0, sizeof ga);
+  ga.skeys = bb.sk;
+  ga.perm = nullptr;
+  ga.values_sorted = 1;
+  ga.n = (u64)n;
+  ga.warp_count = bb.g.warp_count;
+  ga.warp_base = bb.g.warp_base;
+  ga.pack.ncols = 2;
+  ga.pack.c[0].dtype = JFX_U32;
+  ga.pack.c[0].shift = key_bits;
+  ga.pack.c[0].bits = qbits;
+  ga.pack.c[1].dtype = JFX_I32;
+  ga.pack.c[1].shift = 0;
+  ga.pack.c[1].bits = key_bits;
+  ga.pack.c[1].tmin = 0x80000000ull;
+  ga.uniq_out[0] = bb.group_q;
+  ga.uniq_out[1] = group_keys_out;
+  ga.nvals = 1;
+  ValDesc& v = ga.v[0];
+  v.ptr = bb.sv;
+  v.dtype = JFX_F32;
+  v.kind = VK_F;
+  v.aggs = JFX_AGG_SUM | JFX_AGG_COUNT;
+  v.count_dtype = JFX_F32;
+  v.out_sum = group_sums_out;
+  v.out_count = group_counts_out;
+  ga.slot_gid = bb.g.slot_gid;
+  ga.slot_started = bb.g.slot_started;
+  ga.slot_state = bb.g.slot_state;
+  ga.nslots = 2 * bb.g.nwarps;
+  const unsigned blocks = (unsigned)((bb.g.nwarps * 32 + 255) / 256);
+  if (n) {
+    k_group_count<u32><<<blocks, 256, 0, s>>>(ga, bb.g.nwarps), note_launch();
+    JFX_TRY(device_exclusive_scan<u32>(bb.g.warp_count, bb.g.nwarps, bb.g.warp_base, bb.g.total, bb.g.partial, s));
+    JFX_CUDA(cudaMemsetAsync(bb.g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
+    k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, bb.g.nwarps), note_launch();
+    k_group_fixup<<<(unsigned)((ga.nslots + 255) / 256), 256, 0, s>>>(ga), note_launch();
+  } else {
+    JFX_CUDA(cudaMemsetAsync(bb.g.total, 0, sizeof(u32), s));
+  }
+  k_group_offsets<<<gq, 256, 0, s>>>(bb.group_q, bb.g.total, (u32)nq, group_offsets_out), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
+int jfx_batch_status(void* workspace, size_t workspace_bytes, void* stream) {
+  if (!workspace || workspace_bytes < 256) return fail(JFX_ERR_ARG, "null or small workspace");
+  cudaStream_t s = as_stream(stream);
+  u64* host = g_host.get();
+  JFX_TRY(read_back(workspace, sizeof(u32), host, s));  // the error word opens every workspace
+  const u32 e = (u32)host[0];
+  if (e & DERR_BOUNDS) return fail(JFX_ERR_ARG, "a key is outside [0, 2^key_bits) or a query offset decreases");
+  return check_err_word(e);
 }
 
 }  // extern "C"

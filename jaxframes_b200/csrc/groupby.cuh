@@ -53,6 +53,7 @@ struct GroupArgs {
   u32* slot_started;  // [2 * warps]
   u64* slot_state;    // [nvals][4][2 * warps]: sum, min, max, count
   u64 nslots;
+  int values_sorted;  // value columns are already in sorted order (perm unused)
 };
 
 // NaN test on the packed key: a float key column holding the canonical NaN.
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps
     if (lane == 0 && valid && row > 0) kp = sk[row - 1];
     const bool f = valid && (row == 0 || k != kp || packed_has_nan<K>(a.pack, k));
     fm[s] = __ballot_sync(0xffffffffu, f);
-    pr[s] = valid ? a.perm[row] : 0u;
+    pr[s] = valid ? (a.values_sorted ? (u32)row : a.perm[row]) : 0u;
     if (f) {
       // unique key columns of the new group
       const u32 gid = gbase + gcount + __popc(fm[s] & le) - 1u;

@@ -175,20 +175,23 @@ struct FixLists {
   u32 cap_small, cap_medium;
 };
 
+// counts[2] bits: why the fix-up cannot finish (the caller falls back)
+enum : u32 { FIX_LONG_RUN = 1u, FIX_SMALL_FULL = 2u, FIX_MEDIUM_FULL = 4u };
+
 __device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
   const u64 len = e - s;
   if (len > (u64)kFixMaxRun) {
-    atomicExch(&L.counts[2], 1u);
+    atomicOr(&L.counts[2], FIX_LONG_RUN);
     return;
   }
   if (len <= (u64)kFixSmall) {
     const u32 r = atomicAdd(&L.counts[0], 1u);
-    if (r >= L.cap_small) { atomicExch(&L.counts[2], 1u); return; }
+    if (r >= L.cap_small) { atomicOr(&L.counts[2], FIX_SMALL_FULL); return; }
     L.small[2 * r] = (u32)s;
     L.small[2 * r + 1] = (u32)e;
   } else {
     const u32 r = atomicAdd(&L.counts[1], 1u);
-    if (r >= L.cap_medium) { atomicExch(&L.counts[2], 1u); return; }
+    if (r >= L.cap_medium) { atomicOr(&L.counts[2], FIX_MEDIUM_FULL); return; }
     L.medium[2 * r] = (u32)s;
     L.medium[2 * r + 1] = (u32)e;
   }
@@ -196,10 +199,11 @@ __device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
 
 // Lists the runs of equal predicted position that start in this CTA's tile
 // and contain an inversion.
-__global__ void __launch_bounds__(kFindThreads) k_fix_find(const u64* keys, u64 n, const ModelRef* mp,
+__global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals, u64 n, const ModelRef* mp,
                                                            FixLists L) {
   __shared__ u64 sk[kFindTile + 1];
   __shared__ u32 sp[kFindTile + 1];
+  __shared__ u32 sv[kFindTile + 1];
   __shared__ u32 fb[kFindTile / 32 + 2], ib[kFindTile / 32 + 2];
   __shared__ int s_open;
   const ModelRef m = *mp;
@@ -275,7 +279,29 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(const u64* keys, u64 
     }
     bool inv = false;
     for (u32 q = i + 1; q < e && !inv; ++q) inv = (ib[q >> 5] >> (q & 31)) & 1u;
-    if (inv) fix_record(L, base + i, base + e);
+    if (!inv) continue;
+    if (e - i > (u32)kFixSmall) {
+      fix_record(L, base + i, base + e);
+      continue;
+    }
+    // a short run inside the window: stable insertion sort here, then write back
+    for (u32 q = i; q < e; ++q) sv[q] = vals[base + q];
+    for (u32 q = i + 1; q < e; ++q) {
+      const u64 k = sk[q];
+      const u32 v = sv[q];
+      u32 r = q;
+      while (r > i && sk[r - 1] > k) {
+        sk[r] = sk[r - 1];
+        sv[r] = sv[r - 1];
+        --r;
+      }
+      sk[r] = k;
+      sv[r] = v;
+    }
+    for (u32 q = i; q < e; ++q) {
+      keys[base + q] = sk[q];
+      vals[base + q] = sv[q];
+    }
   }
   __syncthreads();
   if (s_open < 0 || threadIdx.x >= 32) return;
@@ -326,7 +352,7 @@ __global__ void k_fix_check(u64 tiles, FixLists L) {
       start = L.last_start[t - k];
       if (start != 0xffffffffu) break;
     }
-    if (start == 0xffffffffu || (u64)inv - start >= (u64)kFixMaxRun) atomicExch(&L.counts[2], 1u);
+    if (start == 0xffffffffu || (u64)inv - start >= (u64)kFixMaxRun) atomicOr(&L.counts[2], FIX_LONG_RUN);
   }
 }
 

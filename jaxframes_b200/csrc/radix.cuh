@@ -40,7 +40,8 @@ struct PassLayout {
   static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
   static constexpr size_t A_BYTES = HIST_BYTES > KEY_BYTES ? HIST_BYTES : KEY_BYTES;
   static constexpr size_t VAL_BYTES = (size_t)TILE * 4;
-  static constexpr size_t SMEM = A_BYTES + VAL_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
+  static constexpr size_t DIG_BYTES = (size_t)TILE * 2;
+  static constexpr size_t SMEM = A_BYTES + VAL_BYTES + DIG_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
 };
 
 // Digit / key modes of one pass.
@@ -50,6 +51,20 @@ enum : int {
   DIG_BITS = 0,   // digit = (key >> shift) & mask
   DIG_MOD = 1,    // digit = key % modulus (hash partition)
   DIG_MODEL = 2,  // digit = (model position of key >> shift) & mask (learned sort)
+  DIG_HASHMOD = 3,  // digit = fmix32(key) % modulus (partition that moves the raw key)
+};
+
+// Segmented passes (batched queries): tiles never straddle a segment, the
+// look-back chains only within a segment and digit offsets are per segment.
+struct SegTables {
+  const u64* row_base;   // [nseg + 1] first row of each segment
+  const u32* tile_base;  // [nseg + 1] first tile id of each segment
+  const u32* tile_seg;   // [tiles] segment of each tile
+  u32 nseg;
+  const u32* total_tiles;  // device: number of real tiles (the grid is an upper bound)
+  int npass_stride;      // passes per segment in the histogram layout
+  int pass_index;        // this pass's index in that layout
+  int key_shift_q;       // > 0: the last pass writes key | (segment << key_shift_q)
 };
 
 // ---- learned-CDF model (fitted in learned.cuh), evaluated inside the passes
@@ -114,6 +129,9 @@ struct PassArgs {
   u32 raw_flags;
   u64 raw_tmin;
   const ModelRef* model; // DIG_MODEL: device-resident model
+  const u32* vals_first; // first pass: payload word per row instead of the row id
+  int segmented;
+  SegTables seg;
   PackDesc pack;
 };
 
@@ -158,9 +176,19 @@ __device__ __forceinline__ u32 hash_row(const PackDesc& pd, size_t row) {
   return fmix32(h);
 }
 
+__device__ __forceinline__ u32 fmix32_d(u32 h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
 template <typename K>
 __device__ __forceinline__ u32 digit_of(K key, int mode, int shift, u32 mask, u32 modulus, const ModelRef& m) {
   if (mode == DIG_MOD) return (u32)key % modulus;
+  if (mode == DIG_HASHMOD) return fmix32_d((u32)key ^ 0x80000000u) % modulus;
   if (mode == DIG_MODEL) return (model_pos(m, (u64)key) >> shift) & mask;
   return (u32)(key >> shift) & mask;
 }
@@ -234,14 +262,15 @@ __device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
 // reading W predecessors' words per round trip, summing aggregates until an
 // inclusive word.  A word not yet published is waited on (bounded).
 template <int W>
-__device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 d, u32 radix, u32* err,
-                                               bool& bad) {
+__device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 tile0, u32 d, u32 radix,
+                                               u32* err, bool& bad) {
   u32 excl = 0;
-  long k = (long)tile - 1;  // next predecessor to read
+  long k = (long)tile - 1;  // next predecessor to read; tile0 publishes inclusive sums
   while (true) {
     u32 v[W];
 #pragma unroll
-    for (int i = 0; i < W; ++i) v[i] = (k - i >= 0) ? ld_relaxed(status + (u64)(k - i) * radix + d) : ST_INC;
+    for (int i = 0; i < W; ++i)
+      v[i] = (k - i >= (long)tile0) ? ld_relaxed(status + (u64)(k - i) * radix + d) : ST_INC;
     int stop = W;
     bool found = false;
     u32 sum = 0;
@@ -287,7 +316,8 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   uint16_t* whist = (uint16_t*)smem;  // [WARPS][RADIX] during ranking
   K* skeys = (K*)smem;                // [TILE] after ranking (aliases whist)
   u32* svals = (u32*)(smem + L::A_BYTES);
-  u32* sexcl = svals + TILE;  // tile digit counts, then the tile's exclusive prefix
+  uint16_t* sdig = (uint16_t*)(svals + TILE);  // digit of each tile-sorted position
+  u32* sexcl = (u32*)(sdig + TILE);  // tile digit counts, then the tile's exclusive prefix
   u32* sbase = sexcl + RADIX; // global position of the tile's first key of each digit
   u32* sscan = sbase + RADIX; // 32 words of block-scan scratch
   u32* sflag = sscan + 32;    // [0] tile id, [1] abort
@@ -300,45 +330,67 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   for (int i = tid; i < WARPS * RADIX / 2; i += THREADS) ((u32*)whist)[i] = 0u;
   __syncthreads();
   const u32 tile = sflag[0];
-  const u64 base = (u64)tile * TILE;
-  const u32 tile_n = (u32)min((u64)TILE, a.n - base);
+  // segment of the tile: rows [seg_row0, seg_row1), tiles from seg_tile0
+  u32 q = 0, seg_tile0 = 0;
+  u64 seg_row0 = 0, seg_row1 = a.n;
+  const u32* bin_base = a.bin_base;
+  if (a.segmented) {
+    if (tile >= *a.seg.total_tiles) return;  // surplus CTA (the grid is an upper bound)
+    q = a.seg.tile_seg[tile];
+    seg_row0 = a.seg.row_base[q];
+    seg_row1 = a.seg.row_base[q + 1];
+    seg_tile0 = a.seg.tile_base[q];
+    bin_base = a.bin_base + ((u64)q * a.seg.npass_stride + a.seg.pass_index) * RADIX;
+  }
+  const u64 base = seg_row0 + (u64)(tile - seg_tile0) * TILE;
+  const u32 tile_n = (u32)min((u64)TILE, seg_row1 - base);
+  const bool first_tile = tile == seg_tile0;
   const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
   ModelRef model;
   if (a.digit_mode == DIG_MODEL) model = *a.model;
   else model.leaves = nullptr;
 
+  // rd[i]: the item's digit in bits [0, 12) (RADIX = not an item), and after
+  // ranking its rank within the warp in bits [12, 32)
   K key[IPT];
-  u32 val[IPT], dig[IPT];
+  u32 val[IPT], rd[IPT];
 #pragma unroll
   for (int i = 0; i < IPT; ++i) {
     const u32 off = warp * 32 * IPT + i * 32 + lane;
-    dig[i] = RADIX;
+    rd[i] = RADIX;
     if (off < tile_n) {
       const u64 idx = base + off;
       if (FIRST) {
         const u64 row = a.gather_idx ? (u64)a.gather_idx[idx] : idx;
         key[i] = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, row) : pack_row<K>(a.pack, row);
-        val[i] = (u32)row;
+        val[i] = a.vals_first ? a.vals_first[row] : (u32)row;
       } else {
         key[i] = ((const K*)a.keys_in)[idx];
         val[i] = a.vals_in[idx];
       }
-      dig[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
+      rd[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
     }
   }
 
   // Stable rank within the warp: lanes holding the same digit are ranked by
   // lane, and items are visited in row order, so equal digits keep row order.
-  u32 rank[IPT];
+  // Peers are found with one ballot per digit bit.
   const u32 lt = lanemask_lt(), gt = lanemask_gt();
   uint16_t* wh = whist + warp * RADIX;
 #pragma unroll
   for (int i = 0; i < IPT; ++i) {
-    const u32 d = dig[i];
-    const u32 peers = __match_any_sync(0xffffffffu, d);
+    const u32 d = rd[i];
     const bool valid = d < (u32)RADIX;
+    u32 peers = __ballot_sync(0xffffffffu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const u32 bit = (d >> b) & 1u;
+      const u32 bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
     const u32 prior = valid ? (u32)wh[d] : 0u;
-    rank[i] = prior + __popc(peers & lt);
+    rd[i] = d | ((prior + __popc(peers & lt)) << 12);
     __syncwarp();
     if (valid && !(peers & gt)) wh[d] = (uint16_t)(prior + __popc(peers));
     __syncwarp();
@@ -363,24 +415,29 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sexcl[d];
     sbase[d] = c;
-    st_relaxed(st + d, (tile == 0 ? ST_INC : ST_AGG) | c);
+    st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | c);
   }
   // Tile-local exclusive prefix and shared-memory sort by digit come before
   // the look-back, which gives earlier tiles time to publish inclusive sums.
   block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);
 
-  u32 pos[IPT];
+  static_assert(TILE <= 8192 && RADIX <= 2048, "position/digit packing");
 #pragma unroll
   for (int i = 0; i < IPT; ++i) {
-    const u32 d = dig[i];
-    pos[i] = d < (u32)RADIX ? sexcl[d] + (u32)whist[warp * RADIX + d] + rank[i] : 0u;
+    const u32 d = rd[i] & 0xfffu;
+    // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
+    rd[i] = d < (u32)RADIX
+                ? 0x80000000u | (d << 13) | (sexcl[d] + (u32)whist[warp * RADIX + d] + (rd[i] >> 12))
+                : 0u;
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < IPT; ++i) {
-    if (dig[i] < (u32)RADIX) {
-      skeys[pos[i]] = key[i];
-      svals[pos[i]] = val[i];
+    if (rd[i] & 0x80000000u) {
+      const u32 p = rd[i] & 0x1fffu;
+      skeys[p] = key[i];
+      svals[p] = val[i];
+      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
     }
   }
 
@@ -390,13 +447,13 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     const u32 c = sbase[d];
     u32 excl = 0;
     bool bad = false;
-    if (tile > 0) {
-      excl = lookback_window<W>(a.status, tile, (u32)d, (u32)RADIX, a.err, bad);
+    if (!first_tile) {
+      excl = lookback_window<W>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, bad);
       st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
     }
     if (bad) sflag[1] = 1u;
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
-    sbase[d] = a.bin_base[d] + excl - sexcl[d];
+    sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
   }
   __syncthreads();
   if (sflag[1]) return;
@@ -404,14 +461,16 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   K* kout = (K*)a.keys_out;
   for (u32 j = tid; j < tile_n; j += THREADS) {
     const K k = skeys[j];
-    const u32 d = digit_of<K>(k, a.digit_mode, a.shift, mask, a.modulus, model);
+    const u32 d = sdig[j];
     u64 g = (u64)(u32)(sbase[d] + j);
-    if (g >= a.n) {  // only reachable if histogram and pass disagree
+    if (g < seg_row0 || g >= seg_row1) {  // only reachable if histogram and pass disagree
       atomicOr(a.err, DERR_BOUNDS);
       continue;
     }
     if (a.reverse) g = a.n - 1 - g;
     if (a.raw_out) store_raw(a.raw_out, a.raw_dtype, g, untransform_int(a.raw_dtype, a.raw_flags, (u64)k + a.raw_tmin));
+    else if (a.segmented && a.seg.key_shift_q)
+      kout[g] = (k & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
     else kout[g] = k;
     a.vals_out[g] = svals[j];
   }
@@ -671,7 +730,7 @@ inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b) {
 }
 
 template <typename K, int RB, bool FIRST>
-inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s) {
+inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles = 0) {
   using L = PassLayout<K, RB>;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
@@ -679,7 +738,7 @@ inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s) {
                                   (int)L::SMEM));
     attr_set = true;
   }
-  int tiles = ceil_div(n, L::TILE);
+  int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
   const long t = timing_begin(s);
   k_onesweep<K, RB, FIRST><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
   if (t >= 0) {

@@ -537,7 +537,9 @@ class ParallelSortMergeJoin:
 def learned_sort(keys, mode: str = "auto"):
     """Learned-CDF partitioned sort of uint64 keys (no reference counterpart):
     ``(sorted_keys, perm int32, learned_used)``, identical to the plain radix
-    sort.  ``mode``: "auto" (learned with plain fallback) or "plain"."""
+    sort.  ``mode``: "auto" (learned with plain fallback) or "plain".
+    ``learned_used`` is 1 for the learned path, 0 for plain, negative for a
+    fallback (-1 model check, -2 run too long, -3 run list full)."""
     k = as_device(keys)
     if k.dtype != torch.uint64:
         raise TypeError(f"learned_sort takes uint64 keys, got {k.dtype}")
@@ -550,7 +552,7 @@ def learned_sort(keys, mode: str = "auto"):
         ws = _lib.workspace(_lib.WS_LEARNED, n, device=k.device)
         check(L.jfx_learned_sort(k.data_ptr(), n, out.data_ptr(), perm.data_ptr(), 0 if mode == "auto" else 1,
                                  ctypes.byref(used), ws.data_ptr(), ws.numel(), _stream()))
-    return out, perm, bool(used.value)
+    return out, perm, int(used.value)
 
 
 def _default_spec(sharding_spec):
