@@ -178,6 +178,61 @@ __device__ __forceinline__ u64 load_t(const ColDesc& c, size_t row) {
   return 0;
 }
 
+// load_t split in two: the transform of a raw element (read with load_raw).
+__device__ __forceinline__ u64 transform_raw(const ColDesc& c, u64 raw) {
+  const bool desc = c.flags & CF_DESC;
+  switch (c.dtype) {
+    case JFX_I32: {
+      u32 x = (u32)raw;
+      if (desc) x = (u32)c.desc_max - x;
+      return x ^ 0x80000000u;
+    }
+    case JFX_I64: {
+      u64 x = raw;
+      if (desc) x = c.desc_max - x;
+      return x ^ 0x8000000000000000ull;
+    }
+    case JFX_U32: {
+      u32 x = (u32)raw;
+      if (desc) x = (u32)c.desc_max - x;
+      return x;
+    }
+    case JFX_U64: return desc ? c.desc_max - raw : raw;
+    case JFX_F32: {
+      float x = __uint_as_float((u32)raw);
+      if (desc) x = -x;
+      return f32_sortable(x);
+    }
+    case JFX_F64: {
+      double x = __longlong_as_double((long long)raw);
+      if (desc) x = -x;
+      return f64_sortable(x);
+    }
+    case JFX_I16: {
+      short x = (short)raw;
+      if (desc) x = (short)((short)c.desc_max - x);
+      return (c.flags & CF_QUIRK) ? (u64)(u32)(int)x : (u64)((u32)(int)x ^ 0x80000000u);
+    }
+    case JFX_I8: {
+      signed char x = (signed char)raw;
+      if (desc) x = (signed char)((signed char)c.desc_max - x);
+      return (c.flags & CF_QUIRK) ? (u64)(u32)(int)x : (u64)((u32)(int)x ^ 0x80000000u);
+    }
+    case JFX_U16: {
+      unsigned short x = (unsigned short)raw;
+      if (desc) x = (unsigned short)((unsigned short)c.desc_max - x);
+      return x;
+    }
+    case JFX_U8: {
+      unsigned char x = (unsigned char)raw;
+      if (desc) x = (unsigned char)((unsigned char)c.desc_max - x);
+      return x;
+    }
+    case JFX_BOOL: return raw ? 1u : 0u;
+  }
+  return 0;
+}
+
 // Inverse of load_t (without CF_DESC) for integer columns: raw bits of the
 // original value, written with the column's element size.
 __host__ __device__ __forceinline__ u64 untransform_int(int dtype, u32 flags, u64 t) {

@@ -89,10 +89,19 @@ __global__ void __launch_bounds__(256) k_group_count(GroupArgs a, u64 nwarps) {
   const K* sk = (const K*)a.skeys;
   const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
   u32 cnt = 0;
-#pragma unroll 4
+  K kv[kGroupIPT], kl[kGroupIPT];
+#pragma unroll
   for (int s = 0; s < kGroupIPT; ++s) {
     const u64 row = wbeg + (u64)s * 32 + lane;
-    const bool f = row < wend && row_flag<K>(a, sk, row);
+    kv[s] = row < wend ? sk[row] : (K)0;
+    kl[s] = (lane == 0 && row < wend && row > 0) ? sk[row - 1] : (K)0;
+  }
+#pragma unroll
+  for (int s = 0; s < kGroupIPT; ++s) {
+    const u64 row = wbeg + (u64)s * 32 + lane;
+    K kp = __shfl_up_sync(0xffffffffu, kv[s], 1);
+    if (lane == 0) kp = kl[s];
+    const bool f = row < wend && (row == 0 || kv[s] != kp || packed_has_nan<K>(a.pack, kv[s]));
     cnt += __popc(__ballot_sync(0xffffffffu, f));
   }
   if (lane == 0) a.warp_count[w] = cnt;
@@ -397,17 +406,24 @@ __global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps
   const u32 le = (2u << lane) - 1u;
   u32 fm[kGroupIPT], pr[kGroupIPT];
   u32 gcount = 0;
+  K kv[kGroupIPT], kl[kGroupIPT];
+#pragma unroll
+  for (int s = 0; s < kGroupIPT; ++s) {  // loads first
+    const u64 row = wbeg + (u64)s * 32 + lane;
+    const bool valid = row < wend;
+    kv[s] = valid ? sk[row] : (K)0;
+    kl[s] = (lane == 0 && valid && row > 0) ? sk[row - 1] : (K)0;
+    pr[s] = valid ? (a.values_sorted ? (u32)row : a.perm[row]) : 0u;
+  }
 #pragma unroll
   for (int s = 0; s < kGroupIPT; ++s) {
     const u64 row = wbeg + (u64)s * 32 + lane;
     const bool valid = row < wend;
-    K k = 0, kp = 0;
-    if (valid) k = sk[row];
+    K k = kv[s], kp = 0;
     kp = __shfl_up_sync(0xffffffffu, k, 1);
-    if (lane == 0 && valid && row > 0) kp = sk[row - 1];
+    if (lane == 0) kp = kl[s];
     const bool f = valid && (row == 0 || k != kp || packed_has_nan<K>(a.pack, k));
     fm[s] = __ballot_sync(0xffffffffu, f);
-    pr[s] = valid ? (a.values_sorted ? (u32)row : a.perm[row]) : 0u;
     if (f) {
       // unique key columns of the new group
       const u32 gid = gbase + gcount + __popc(fm[s] & le) - 1u;

@@ -65,11 +65,17 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_count(const K* A, u64 na,
   if (in_smem)
     for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = B[wlo + i];
   __syncthreads();
+  K xs[kJoinIPT];
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 i = a0 + (u64)k * kJoinThreads + threadIdx.x;
+    xs[k] = i < a1 ? A[i] : (K)0;
+  }
 #pragma unroll
   for (int k = 0; k < kJoinIPT; ++k) {
     const u64 i = a0 + (u64)k * kJoinThreads + threadIdx.x;
     if (i >= a1) break;
-    const K x = A[i];
+    const K x = xs[k];
     u64 l, h;
     if (in_smem) {
       l = lower_bound_g<K>(win, 0, wn, x);
@@ -133,20 +139,44 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_expand_inner(const u64* o
   if (in_smem)
     for (u64 i = threadIdx.x; i < wn; i += kJoinThreads) win[i] = off[i0 + i];
   __syncthreads();
+  // three rounds so each round's loads are all in flight together
+  u64 ii[kJoinIPT], jj[kJoinIPT];
 #pragma unroll
   for (int k = 0; k < kJoinIPT; ++k) {
     const u64 o = o0 + (u64)k * kJoinThreads + threadIdx.x;
-    if (o >= o1) break;
+    ii[k] = 0;
+    jj[k] = 0;
+    if (o >= o1) continue;
     u64 r;
     if (in_smem) r = upper_bound_g<u64>(win, 0, wn, o) - 1;
     else r = upper_bound_g<u64>(off + i0, 0, wn, o) - 1;
-    const u64 i = i0 + r;
-    const u64 base = in_smem ? win[r] : off[i];
-    const u64 j = (u64)lo[i] + (o - base);
-    const u32 ra = pA[i];
-    a_out[o] = (int32_t)ra;
-    b_out[o] = (int32_t)pB[j];
-    write_join_key<K>(ko, o, skA[i], ra);
+    ii[k] = i0 + r;
+    jj[k] = o - (in_smem ? win[r] : off[i0 + r]);  // offset inside the row's run
+  }
+  u32 ra[kJoinIPT], lo_k[kJoinIPT];
+  K kk[kJoinIPT];
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 o = o0 + (u64)k * kJoinThreads + threadIdx.x;
+    if (o >= o1) continue;
+    ra[k] = pA[ii[k]];
+    lo_k[k] = lo[ii[k]];
+    kk[k] = skA[ii[k]];
+  }
+  u32 rb[kJoinIPT];
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 o = o0 + (u64)k * kJoinThreads + threadIdx.x;
+    if (o >= o1) continue;
+    rb[k] = pB[(u64)lo_k[k] + jj[k]];
+  }
+#pragma unroll
+  for (int k = 0; k < kJoinIPT; ++k) {
+    const u64 o = o0 + (u64)k * kJoinThreads + threadIdx.x;
+    if (o >= o1) continue;
+    a_out[o] = (int32_t)ra[k];
+    b_out[o] = (int32_t)rb[k];
+    write_join_key<K>(ko, o, kk[k], ra[k]);
   }
 }
 
@@ -167,6 +197,32 @@ __global__ void __launch_bounds__(256) k_join_expand_first(u64 na, const u32* lo
 // out[i] = src[idx[i]] converted to out_dtype; idx < 0 -> NaN (float out) or -1.
 __global__ void __launch_bounds__(256) k_gather(const void* src, int sdt, u64 n_src, const int32_t* idx, u64 n,
                                                void* out, int odt) {
+  // same-dtype fast path: indices of U items, then their values, then stores
+  constexpr int U = 8;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  if (odt == sdt) {
+    for (u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * U) {
+      int32_t r[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 i = i0 + (u64)u * stride;
+        r[u] = i < n ? idx[i] : -1;
+      }
+      u64 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = (r[u] >= 0 && (u64)r[u] < n_src) ? load_raw(src, sdt, (u64)r[u]) : 0ull;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 i = i0 + (u64)u * stride;
+        if (i >= n) break;
+        if (r[u] >= 0 && (u64)r[u] < n_src) store_raw(out, odt, i, v[u]);
+        else if (odt == JFX_F32) ((float*)out)[i] = __int_as_float(0x7fc00000);
+        else if (odt == JFX_F64) ((double*)out)[i] = __longlong_as_double(0x7ff8000000000000ll);
+        else store_raw(out, odt, i, ~0ull);
+      }
+    }
+    return;
+  }
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
     const int32_t r = idx[i];
     if (r < 0 || (u64)r >= n_src) {

@@ -352,23 +352,49 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
 
   // rd[i]: the item's digit in bits [0, 12) (RADIX = not an item), and after
   // ranking its rank within the warp in bits [12, 32)
+  // Issue every load of the tile before using any of them (memory-level
+  // parallelism: one DRAM round trip per tile, not one per item).
   K key[IPT];
   u32 val[IPT], rd[IPT];
+  const bool full = tile_n == (u32)TILE;
+  const bool simple_first = FIRST && a.pack.ncols == 1 && a.key_mode == KEY_PACK && !a.gather_idx;
+  if (!FIRST || simple_first) {
+    u64 raw[IPT];
 #pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    const u32 off = warp * 32 * IPT + i * 32 + lane;
-    rd[i] = RADIX;
-    if (off < tile_n) {
+    for (int i = 0; i < IPT; ++i) {
+      const u32 off = warp * 32 * IPT + i * 32 + lane;
       const u64 idx = base + off;
-      if (FIRST) {
+      if (full || off < tile_n) {
+        if (FIRST) raw[i] = load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, idx);
+        else key[i] = ((const K*)a.keys_in)[idx];
+        if (!FIRST) val[i] = a.vals_in[idx];
+        else val[i] = a.vals_first ? a.vals_first[idx] : (u32)idx;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 off = warp * 32 * IPT + i * 32 + lane;
+      rd[i] = RADIX;
+      if (full || off < tile_n) {
+        if (FIRST) key[i] = (K)(transform_raw(a.pack.c[0], raw[i]) - a.pack.c[0].tmin) << a.pack.c[0].shift;
+        rd[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 off = warp * 32 * IPT + i * 32 + lane;
+      if (off < tile_n) {
+        const u64 idx = base + off;
         const u64 row = a.gather_idx ? (u64)a.gather_idx[idx] : idx;
         key[i] = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, row) : pack_row<K>(a.pack, row);
         val[i] = a.vals_first ? a.vals_first[row] : (u32)row;
-      } else {
-        key[i] = ((const K*)a.keys_in)[idx];
-        val[i] = a.vals_in[idx];
       }
-      rd[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
+    }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 off = warp * 32 * IPT + i * 32 + lane;
+      rd[i] = off < tile_n ? digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model) : (u32)RADIX;
     }
   }
 
@@ -506,8 +532,32 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
   if (a.digit_mode == DIG_MODEL) model = *a.model;
   else model.leaves = nullptr;
   const u64 stride = (u64)gridDim.x * blockDim.x;
-  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < a.n; r += stride) {
-    const K k = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, r) : pack_row<K>(a.pack, r);
+  constexpr int U = 8;  // rows per thread per step, loads issued together
+  const bool simple = a.pack.ncols == 1 && a.key_mode == KEY_PACK;
+  for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < a.n; r0 += stride * U) {
+    K kk[U];
+    if (simple) {
+      u64 raw[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        raw[u] = r < a.n ? load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, r) : 0ull;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        kk[u] = (K)(transform_raw(a.pack.c[0], raw[u]) - a.pack.c[0].tmin) << a.pack.c[0].shift;
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        kk[u] = r < a.n ? (a.key_mode == KEY_HASH ? (K)hash_row(a.pack, r) : pack_row<K>(a.pack, r)) : (K)0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+    const u64 r = r0 + (u64)u * stride;
+    if (r >= a.n) break;
+    const K k = kk[u];
     if (a.digit_mode == DIG_MODEL) {
       const u32 pos = model_pos(model, (u64)k);
 #pragma unroll
@@ -523,6 +573,7 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
       const u32 d = digit_of<K>(k, a.digit_mode, a.shift[p], mask[p], a.modulus, model);
       atomicAdd(&sh[p * RADIX + d], 1u);
       if (p == 0 && a.targets) a.targets[r] = d;
+    }
     }
   }
   __syncthreads();
@@ -553,13 +604,37 @@ __global__ void __launch_bounds__(256) k_minmax(PackDesc pd, u64 n, u64* out) {
     mx[j] = 0ull;
   }
   const u64 stride = (u64)gridDim.x * blockDim.x;
-  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+  constexpr int U = 8;
+  if (pd.ncols == 1) {
+    for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += stride * U) {
+      u64 raw[U];
 #pragma unroll
-    for (int j = 0; j < kMaxCols; ++j) {
-      if (j >= pd.ncols) break;
-      const u64 t = load_t(pd.c[j], r);
-      mn[j] = t < mn[j] ? t : mn[j];
-      mx[j] = t > mx[j] ? t : mx[j];
+      for (int u = 0; u < U; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        raw[u] = r < n ? load_raw(pd.c[0].ptr, pd.c[0].dtype, r) : 0ull;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (r0 + (u64)u * stride >= n) break;
+        const u64 t = transform_raw(pd.c[0], raw[u]);
+        mn[0] = t < mn[0] ? t : mn[0];
+        mx[0] = t > mx[0] ? t : mx[0];
+      }
+    }
+  } else {
+    for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += stride * 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        if (r >= n) break;
+#pragma unroll
+        for (int j = 0; j < kMaxCols; ++j) {
+          if (j >= pd.ncols) break;
+          const u64 t = load_t(pd.c[j], r);
+          mn[j] = t < mn[j] ? t : mn[j];
+          mx[j] = t > mx[j] ? t : mx[j];
+        }
+      }
     }
   }
 #pragma unroll
@@ -602,7 +677,7 @@ __global__ void k_fill_keys(K* out, u64 n) {
 // ----------------------------------------------------------- host driver ---
 // Thread-local tuning (jfx_set_tuning): widest radix digit of a pass.
 struct Tuning {
-  int max_digit_bits = 11;
+  int max_digit_bits = 8;
 };
 extern thread_local Tuning g_tuning;
 
