@@ -86,6 +86,7 @@ static void carve_lexsort(Arena& ar, u64 n, Common& c, SortBuffers& b, u32** tmp
 struct GroupBuffers {
   void* sk;
   u32* perm;
+  u32* words[kMaxWords];  // sorted payload words when values are carried
   u32* warp_count;
   u32* warp_base;
   u32* partial;
@@ -96,9 +97,11 @@ struct GroupBuffers {
   u64 nwarps;
 };
 static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b, GroupBuffers& g) {
-  carve_sort(ar, n, c, b);
+  take_common(ar, c);
+  take_sort_buffers(ar, n, b, kMaxWords);
   g.sk = ar.take<u64>(n ? n : 1);
   g.perm = ar.take<u32>(n ? n : 1);
+  for (int w = 0; w < kMaxWords; ++w) g.words[w] = ar.take<u32>(n ? n : 1);
   g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
   g.warp_count = ar.take<u32>(g.nwarps + 1);
   g.warp_base = ar.take<u32>(g.nwarps + 1);
@@ -213,10 +216,13 @@ static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBu
   l.tiles = (n + kFindTile - 1) / kFindTile;
   l.fix.cap_small = (u32)(n / 8 + 64);
   l.fix.cap_medium = (u32)(n / 512 + 64);
+  l.fix.cap_long = (u32)(n / kFixMaxRun + 64);
   l.fix.small = ar.take<u32>(2 * (u64)l.fix.cap_small);
   l.fix.medium = ar.take<u32>(2 * (u64)l.fix.cap_medium);
+  l.fix.lng = ar.take<u32>(2 * (u64)l.fix.cap_long);
   l.fix.counts = ar.take<u32>(8);
   l.fix.last_start = ar.take<u32>(l.tiles + 1);
+  l.fix.scanned_to = ar.take<u32>(l.tiles + 1);
   l.fix.carried_inv = ar.take<u32>(l.tiles + 1);
 }
 
@@ -586,16 +592,53 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   JFX_TRY(plan_keys(kp, (u64)n, c.mm, s));
   if (kp.total_bits > 64)
     return fail(JFX_ERR_CAPACITY, "group keys need %d packed bits; at most 64 are supported", kp.total_bits);
+  // Carry the value columns through the sort when they fit in the payload
+  // words (4- and 8-byte values, plus the row id when a key is a float):
+  // the reduce then reads them in sorted order instead of gathering.
+  int words = kp.pack.nan_cols ? 1 : 0;
+  bool carry = true;
+  for (int i = 0; i < nvalues; ++i) {
+    const int sz = dtype_size(values[i].dtype);
+    if (sz < 4) carry = false;
+    words += sz == 8 ? 2 : 1;
+  }
+  if (words > kMaxWords || nvalues == 0) carry = false;
   RadixRequest rq;
   rq.pack = kp.pack;
   rq.total_bits = kp.total_bits;
   rq.key64 = kp.total_bits > 32;
   rq.perm_out = g.perm;
   rq.keys_out = g.sk;
+  int rowid_word = -1;
+  if (carry) {
+    rq.total_bits = std::max(1, kp.total_bits);  // one pass even for constant keys
+    int w = 0;
+    for (int i = 0; i < nvalues; ++i) {
+      const int sz = dtype_size(values[i].dtype);
+      ValDesc& d = ga.v[i];
+      d.carried = 1;
+      rq.pfirst[w] = PayloadSrc{(const unsigned char*)values[i].data, (u32)sz, 0u};
+      rq.vout_final[w] = g.words[w];
+      d.ptr = g.words[w++];
+      if (sz == 8) {
+        rq.pfirst[w] = PayloadSrc{(const unsigned char*)values[i].data, 8u, 4u};
+        rq.vout_final[w] = g.words[w];
+        d.ptr_hi = g.words[w++];
+      }
+    }
+    if (kp.pack.nan_cols) {
+      rowid_word = w;
+      rq.pfirst[w] = PayloadSrc{nullptr, 0u, 0u};
+      rq.vout_final[w] = g.words[w];
+      ++w;
+    }
+    rq.nwords = w;
+  }
   JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
 
   ga.skeys = g.sk;
-  ga.perm = g.perm;
+  ga.perm = carry ? (rowid_word >= 0 ? g.words[rowid_word] : nullptr) : g.perm;
+  ga.values_sorted = carry ? 1 : 0;
   ga.n = (u64)n;
   ga.warp_count = g.warp_count;
   ga.warp_base = g.warp_base;
@@ -961,7 +1004,10 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   JFX_CUDA(cudaMemsetAsync(l.flags, 0x01, 8 * sizeof(u32), s));
   k_leaf_bounds<<<g, 256, 0, s>>>(l.ssorted, l.s, l.model, l.first, l.last), note_launch();
   k_leaf_fit<<<kLeaves * 32 / 256, 256, 0, s>>>(l.ssorted, l.first, l.last, l.fit), note_launch();
-  k_leaf_finalize<<<1, 1024, 0, s>>>(l.ssorted, l.s, N, l.first, l.last, l.fit, l.leaves, l.flags), note_launch();
+  // predicted positions range over [0, 4n): finer than one slot per row, so
+  // distinct keys share a position less often
+  const u64 npos = 4 * N;
+  k_leaf_finalize<<<1, 1024, 0, s>>>(l.ssorted, l.s, npos, l.first, l.last, l.fit, l.leaves, l.flags), note_launch();
   JFX_CUDA(cudaGetLastError());
   // 3. radix passes over the predicted position
   {
@@ -971,7 +1017,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     rq.pack.c[0].bits = 64;
     rq.digit_mode = DIG_MODEL;
     rq.model = l.model;
-    rq.total_bits = std::max(1, bit_length(N - 1));
+    rq.total_bits = std::max(1, bit_length(npos - 1));
     rq.key64 = true;
     rq.perm_out = (u32*)perm_out;
     rq.keys_out = sorted_keys_out;
@@ -990,6 +1036,8 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     }
   }
   k_fix_medium<<<device_sm_count(), kFixMedThreads, kFixMediumSmem, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
+  // long runs: the sort's ping-pong buffers are free now and serve as scratch
+  k_fix_long<<<device_sm_count(), kFixMedThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, (u64*)b.keys[0], b.vals[0][0], l.fix), note_launch();
   JFX_CUDA(cudaGetLastError());
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host + 1, l.flags, sizeof(u32), cudaMemcpyDeviceToHost, s));
@@ -1105,11 +1153,12 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   a.digit_mode = DIG_HASHMOD;
   a.modulus = (u32)num_partitions;
   a.width = RB;
-  a.vals_first = (const u32*)values;
+  a.pfirst[0].ptr = (const unsigned char*)values;
+  a.pfirst[0].stride = 4;
   a.raw_out = part_keys_out;
   a.raw_dtype = JFX_I32;
   a.keys_out = bb.keys[0];
-  a.vals_out = (u32*)part_values_out;
+  a.vout[0] = (u32*)part_values_out;
   a.status = bb.status[0];
   a.status_next = bb.status[1];
   a.tile_counter = bb.counters;
@@ -1126,15 +1175,15 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   for (int p = 1; p <= npk; ++p) {
     const bool last = p == npk;
     PassArgs b = a;
-    b.vals_first = nullptr;
+    b.pfirst[0].ptr = nullptr;
     b.raw_out = nullptr;
     b.digit_mode = DIG_BITS;
     b.shift = shift[p];
     b.width = width[p];
     b.keys_in = kin;
-    b.vals_in = vin;
+    b.vin[0] = vin;
     b.keys_out = last ? bb.sk : bb.keys[p & 1];
-    b.vals_out = last ? bb.sv : bb.vals[p & 1];
+    b.vout[0] = last ? bb.sv : bb.vals[p & 1];
     b.status = bb.status[p & 1];
     b.status_next = last ? nullptr : bb.status[(p + 1) & 1];
     b.tile_counter = bb.counters + p;
@@ -1142,7 +1191,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
     b.seg.key_shift_q = last ? key_bits : 0;
     JFX_TRY((launch_pass<u32, RB, false>(b, (u64)n, s, bb.max_tiles)));
     kin = (const u32*)b.keys_out;
-    vin = b.vals_out;
+    vin = b.vout[0];
   }
   // groupby sum and count over the whole batch on (query, key) composite keys
   GroupArgs ga;

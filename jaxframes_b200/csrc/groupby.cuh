@@ -26,6 +26,8 @@ enum : int { VK_F = 0, VK_I = 1, VK_U = 2 };
 
 struct ValDesc {
   const void* ptr;
+  const void* ptr_hi;  // carried 8-byte values: high words (ptr: low words)
+  int carried;         // values were carried through the sort as u32 words
   int dtype;
   int kind;
   u32 aggs;
@@ -162,6 +164,16 @@ __device__ __forceinline__ Agg<KIND> agg_combine(const Agg<KIND>& a, const Agg<K
 // The row's value as the 64-bit word the partial state holds.
 template <int KIND>
 __device__ __forceinline__ u64 value_word(const ValDesc& v, u64 row) {
+  if (v.carried) {
+    const u32 lo = __ldg((const u32*)v.ptr + row);
+    if (dtype_size(v.dtype) == 8) {
+      const u64 w = (u64)lo | ((u64)__ldg((const u32*)v.ptr_hi + row) << 32);
+      return KIND == VK_F ? w : w;  // f64 bits / i64 / u64 as stored
+    }
+    if (KIND == VK_F) return __double_as_longlong((double)__uint_as_float(lo));
+    if (KIND == VK_I) return (u64)(long long)(int)lo;
+    return (u64)lo;
+  }
   if (KIND == VK_F) {
     const double x = v.dtype == JFX_F32 ? (double)__ldg((const float*)v.ptr + row) : __ldg((const double*)v.ptr + row);
     return __double_as_longlong(x);
@@ -431,7 +443,9 @@ __global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps
         const ColDesc& c = a.pack.c[j];
         if (!a.uniq_out[j]) continue;
         if (dtype_is_float(c.dtype)) {
-          store_raw(a.uniq_out[j], c.dtype, gid, load_raw(c.ptr, c.dtype, pr[s]));
+          // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
+          const u32 krow = a.perm ? a.perm[row] : (u32)row;
+          store_raw(a.uniq_out[j], c.dtype, gid, load_raw(c.ptr, c.dtype, krow));
         } else {
           const u64 field = c.bits ? (((u64)k >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull))) : 0ull;
           store_raw(a.uniq_out[j], c.dtype, gid, untransform_int(c.dtype, c.flags, field + c.tmin));

@@ -119,6 +119,8 @@ __global__ void __launch_bounds__(256) k_leaf_fit(const u64* sx, const u32* firs
 __global__ void __launch_bounds__(1024) k_leaf_finalize(const u64* sx, u64 s, u64 n, const u32* first,
                                                         const u32* last, const double* fit, Leaf* leaves,
                                                         u32* ok) {
+  // n here is the range of predicted positions (a multiple of the row count:
+  // finer positions make distinct keys collide less often)
   __shared__ u32 nf[kLeaves];
   const double scale = (double)n / (double)s;
   for (int l = threadIdx.x; l < kLeaves; l += 1024) nf[l] = first[l] == 0xffffffffu ? (u32)s : first[l];
@@ -163,16 +165,19 @@ __global__ void __launch_bounds__(1024) k_leaf_finalize(const u64* sx, u64 s, u6
 
 // ------------------------------------------------------------------ fix-up ---
 constexpr int kFindTile = 2048, kFindThreads = 256;
-constexpr int kFixMaxRun = 6144;   // longest run the block sort takes
+constexpr int kFixMaxRun = 6144;   // longest run the shared-memory block sort takes
+constexpr u32 kFixLongMax = 1u << 20;  // longest run the global-memory sort takes
 constexpr int kFixSmall = 32;      // runs up to this length: one warp
 
 struct FixLists {
   u32* small;       // [cap_small][2] (start, end)
   u32* medium;      // [cap_medium][2]
-  u32* counts;      // [0] small, [1] medium, [2] overflow flag
+  u32* lng;         // [cap_long][2]
+  u32* counts;      // [0] small, [1] medium, [2] overflow flag, [3] long
   u32* last_start;  // [tiles] last run start in the tile, or ~0
   u32* carried_inv; // [tiles] first inversion of the run carried into the tile, or ~0
-  u32 cap_small, cap_medium;
+  u32* scanned_to;  // [tiles] position up to which the tile's last run was scanned
+  u32 cap_small, cap_medium, cap_long;
 };
 
 // counts[2] bits: why the fix-up cannot finish (the caller falls back)
@@ -180,8 +185,15 @@ enum : u32 { FIX_LONG_RUN = 1u, FIX_SMALL_FULL = 2u, FIX_MEDIUM_FULL = 4u };
 
 __device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
   const u64 len = e - s;
-  if (len > (u64)kFixMaxRun) {
+  if (len > (u64)kFixLongMax) {
     atomicOr(&L.counts[2], FIX_LONG_RUN);
+    return;
+  }
+  if (len > (u64)kFixMaxRun) {
+    const u32 r = atomicAdd(&L.counts[3], 1u);
+    if (r >= L.cap_long) { atomicOr(&L.counts[2], FIX_MEDIUM_FULL); return; }
+    L.lng[2 * r] = (u32)s;
+    L.lng[2 * r + 1] = (u32)e;
     return;
   }
   if (len <= (u64)kFixSmall) {
@@ -304,15 +316,24 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
     }
   }
   __syncthreads();
+  if (threadIdx.x == 0) L.scanned_to[blockIdx.x] = (u32)t1;
   if (s_open < 0 || threadIdx.x >= 32) return;
-  // the last run of the tile: scan on past the tile, 32 keys at a time
+  // the last run of the tile continues past it: scan on, 32 keys at a time.
+  // A run whose keys are all equal so far holds no inversion; past
+  // kFixMaxRun such a run is left to k_fix_check.  A run with distinct keys
+  // is scanned to its end (at most kFixLongMax).
   const u32 i = (u32)s_open;
   const u32 p0 = sp[i];
-  bool inv = false;
-  for (u32 q = i + 1; q < len; ++q) inv |= (ib[q >> 5] >> (q & 31)) & 1u;
+  const u64 k0 = sk[i];
+  bool inv = false, distinct = false;
+  for (u32 q = i + 1; q < len; ++q) {
+    inv |= (ib[q >> 5] >> (q & 31)) & 1u;
+    distinct |= sk[q] != k0;
+  }
   u64 prev_key = sk[len - 1];
   u64 pos = t1;
   u64 e = n;
+  bool ended = false;
   while (pos < n) {
     const u64 q = pos + lane;
     const bool in = q < n;
@@ -321,24 +342,28 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
     const u32 bs = __ballot_sync(0xffffffffu, same);
     const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
     const u64 km = lane == 0 ? prev_key : kp;
-    // positions of this chunk that still belong to the run: a prefix of lanes
     const u32 run_lanes = ~bs ? (u32)(__ffs(~bs) - 1) : 32u;
-    const bool vi = (u32)lane < run_lanes && km > k;
-    inv |= __ballot_sync(0xffffffffu, vi) != 0;
+    const bool mine = (u32)lane < run_lanes;
+    inv |= __ballot_sync(0xffffffffu, mine && km > k) != 0;
+    distinct |= __ballot_sync(0xffffffffu, mine && k != k0) != 0;
     if (run_lanes < 32) {
       e = pos + run_lanes;
+      ended = true;
       break;
     }
     prev_key = __shfl_sync(0xffffffffu, k, 31);
     pos += 32;
-    if (pos - (base + i) > (u64)kFixMaxRun) {
+    const u64 scanned = pos - (base + i);
+    if ((!distinct && !inv && scanned > (u64)kFixMaxRun) || scanned > (u64)kFixLongMax) {
       e = pos;
       break;
     }
   }
-  // a run longer than the window: an inversion seen here cannot be fixed
-  // (overflow); one past the window is caught by k_fix_check
-  if (lane == 0 && inv) fix_record(L, base + i, e);
+  if (pos >= n) ended = true;
+  if (lane == 0) {
+    L.scanned_to[blockIdx.x] = (u32)(ended ? n : e);
+    if (inv) fix_record(L, base + i, ended ? e : (u64)n + kFixLongMax);  // unended + inversion: too long
+  }
 }
 
 // A run carried into a tile with an inversion the run's owner did not scan
@@ -348,11 +373,19 @@ __global__ void k_fix_check(u64 tiles, FixLists L) {
     const u32 inv = L.carried_inv[t];
     if (inv == 0xffffffffu) continue;
     u32 start = 0xffffffffu;
-    for (u64 k = 1; k <= t && k <= (u64)(kFixMaxRun / kFindTile + 2); ++k) {
+    for (u64 k = 1; k <= t && k <= (u64)(kFixLongMax / kFindTile + 2); ++k) {
       start = L.last_start[t - k];
       if (start != 0xffffffffu) break;
     }
-    if (start == 0xffffffffu || (u64)inv - start >= (u64)kFixMaxRun) atomicOr(&L.counts[2], FIX_LONG_RUN);
+    // the owner of the run is the nearest earlier tile with a run start; it
+    // scanned the run up to scanned_to (its inversions there are handled)
+    u32 owner_scan = 0;
+    for (u64 k = 1; k <= t && k <= (u64)(kFixLongMax / kFindTile + 2); ++k)
+      if (L.last_start[t - k] != 0xffffffffu) {
+        owner_scan = L.scanned_to[t - k];
+        break;
+      }
+    if (start == 0xffffffffu || inv >= owner_scan) atomicOr(&L.counts[2], FIX_LONG_RUN);
   }
 }
 
@@ -470,6 +503,99 @@ __global__ void __launch_bounds__(kFixMedThreads) k_fix_medium(u64* keys, u32* v
     for (u32 j = tid; j < m; j += kFixMedThreads) {
       keys[s + j] = src[j];
       vals[s + j] = sv[isrc[j]];
+    }
+    __syncthreads();
+  }
+}
+
+// Sorts each long run (kFixMaxRun < length <= kFixLongMax) with one CTA: a
+// stable LSD radix sort of 8-bit digits of key - min, ping-ponging between
+// the run's place in the output and the same positions of a scratch array.
+__global__ void __launch_bounds__(kFixMedThreads) k_fix_long(u64* keys, u32* vals, u64* tkeys, u32* tvals,
+                                                             FixLists L) {
+  __shared__ u32 hist[256];
+  __shared__ u32 wh[8][256];
+  __shared__ u64 s_min, s_max;
+  __shared__ u32 scan_scratch[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32 cnt = min(L.counts[3], L.cap_long);
+  for (u32 r = blockIdx.x; r < cnt; r += gridDim.x) {
+    const u32 s = L.lng[2 * r], e = L.lng[2 * r + 1];
+    if (tid == 0) {
+      s_min = ~0ull;
+      s_max = 0;
+    }
+    __syncthreads();
+    u64 lmin = ~0ull, lmax = 0;
+    for (u32 j = s + tid; j < e; j += kFixMedThreads) {
+      const u64 k = keys[j];
+      lmin = k < lmin ? k : lmin;
+      lmax = k > lmax ? k : lmax;
+    }
+    atomicMin(&s_min, lmin);
+    atomicMax(&s_max, lmax);
+    __syncthreads();
+    const u64 mn = s_min;
+    const int bits = bit_length(s_max - mn);
+    u64 *ks = keys, *kd = tkeys;
+    u32 *vs = vals, *vd = tvals;
+    for (int sh = 0; sh < bits; sh += 8) {
+      for (int i = tid; i < 256; i += kFixMedThreads) hist[i] = 0;
+      __syncthreads();
+      for (u32 j = s + tid; j < e; j += kFixMedThreads) atomicAdd(&hist[(u32)(((ks[j] - mn) >> sh) & 255u)], 1u);
+      __syncthreads();
+      block_exclusive_scan<kFixMedThreads, 256>(hist, scan_scratch);  // hist: running base per digit
+      // chunks of 256 rows in order; inside a chunk, warp w takes rows
+      // [w*32, w*32+32) so warps are in row order too
+      const u32 lt = lanemask_lt();
+      for (u32 c0 = s; c0 < e; c0 += kFixMedThreads) {
+        for (int i = tid; i < 8 * 256; i += kFixMedThreads) (&wh[0][0])[i] = 0;
+        __syncthreads();
+        const u32 j = c0 + tid;
+        const bool in = j < e;
+        const u64 k = in ? ks[j] : 0;
+        const u32 v = in ? vs[j] : 0;
+        const u32 d = in ? (u32)(((k - mn) >> sh) & 255u) : 256u;
+        u32 peers = __ballot_sync(0xffffffffu, in);
+        if (!in) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const u32 bit = (d >> b) & 1u;
+          const u32 bb = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? bb : ~bb;
+        }
+        const u32 rank = __popc(peers & lt);
+        if (in && !(peers & lanemask_gt())) wh[warp][d] = __popc(peers);
+        __syncthreads();
+        // offset of this warp's first row of digit d: earlier warps of the chunk
+        u32 before = 0;
+        if (in)
+          for (int w = 0; w < warp; ++w) before += wh[w][d];
+        if (in) {
+          const u32 dst = s + hist[d] + before + rank;
+          kd[dst] = k;
+          vd[dst] = v;
+        }
+        __syncthreads();
+        if (tid < 256) {
+          u32 tot = 0;
+          for (int w = 0; w < 8; ++w) tot += wh[w][tid];
+          hist[tid] += tot;
+        }
+        __syncthreads();
+      }
+      u64* tk = ks;
+      ks = kd;
+      kd = tk;
+      u32* tv = vs;
+      vs = vd;
+      vd = tv;
+    }
+    if (ks != keys) {  // odd number of passes: the run ended up in the scratch
+      for (u32 j = s + tid; j < e; j += kFixMedThreads) {
+        keys[j] = ks[j];
+        vals[j] = vs[j];
+      }
     }
     __syncthreads();
   }

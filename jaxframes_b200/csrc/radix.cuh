@@ -32,17 +32,34 @@ struct RadixCfg {
   static constexpr int IPT = 16;
 };
 
-template <typename K, int RB>
+constexpr int kMaxWords = 4;  // payload words a pass can carry per row
+
+template <typename K, int RB, int NW = 1>
 struct PassLayout {
   static constexpr int THREADS = RadixCfg<RB>::THREADS, IPT = RadixCfg<RB>::IPT;
   static constexpr int RADIX = 1 << RB, WARPS = THREADS / 32, TILE = THREADS * IPT;
   static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 2;
   static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
   static constexpr size_t A_BYTES = HIST_BYTES > KEY_BYTES ? HIST_BYTES : KEY_BYTES;
-  static constexpr size_t VAL_BYTES = (size_t)TILE * 4;
+  static constexpr size_t PAY_BYTES = (size_t)NW * TILE * 4;  // payload staged in row order
+  static constexpr size_t IDX_BYTES = (size_t)TILE * 2;       // sorted slot -> staging slot
   static constexpr size_t DIG_BYTES = (size_t)TILE * 2;
-  static constexpr size_t SMEM = A_BYTES + VAL_BYTES + DIG_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
+  static constexpr size_t SMEM = A_BYTES + PAY_BYTES + IDX_BYTES + DIG_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
 };
+
+// Where the first pass reads payload word w of row r: *(u32*)(ptr + r*stride + off);
+// a null ptr means the row id itself.
+struct PayloadSrc {
+  const unsigned char* ptr;
+  u32 stride;
+  u32 off;
+};
+
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Digit / key modes of one pass.
 enum : int {
@@ -110,9 +127,10 @@ __device__ __forceinline__ u32 model_pos(const ModelRef& m, u64 x) {
 
 struct PassArgs {
   const void* keys_in;   // K[n] (not read by the first pass)
-  const u32* vals_in;    // u32[n] (not read by the first pass)
+  const u32* vin[kMaxWords];   // payload words u32[n] each (not read by the first pass)
   void* keys_out;        // K[n]
-  u32* vals_out;         // u32[n]
+  u32* vout[kMaxWords];  // payload words out
+  PayloadSrc pfirst[kMaxWords];  // first pass: payload word sources
   const u32* bin_base;   // [RADIX] exclusive global digit offsets of this pass
   u32* status;           // [tiles][RADIX] look-back words of this pass (zeroed)
   u32* status_next;      // [tiles][RADIX] to clear for the following pass, or null
@@ -129,7 +147,6 @@ struct PassArgs {
   u32 raw_flags;
   u64 raw_tmin;
   const ModelRef* model; // DIG_MODEL: device-resident model
-  const u32* vals_first; // first pass: payload word per row instead of the row id
   int segmented;
   SegTables seg;
   PackDesc pack;
@@ -307,20 +324,21 @@ __device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 
   }
 }
 
-template <typename K, int RB, bool FIRST>
+template <typename K, int RB, bool FIRST, int NW>
 __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
-  using L = PassLayout<K, RB>;
+  using L = PassLayout<K, RB, NW>;
   constexpr int THREADS = L::THREADS, IPT = L::IPT, RADIX = L::RADIX, WARPS = L::WARPS,
                 TILE = L::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* whist = (uint16_t*)smem;  // [WARPS][RADIX] during ranking
   K* skeys = (K*)smem;                // [TILE] after ranking (aliases whist)
-  u32* svals = (u32*)(smem + L::A_BYTES);
-  uint16_t* sdig = (uint16_t*)(svals + TILE);  // digit of each tile-sorted position
+  u32* spay = (u32*)(smem + L::A_BYTES);                 // [NW][TILE] payload, row order
+  uint16_t* sidx = (uint16_t*)(smem + L::A_BYTES + L::PAY_BYTES);  // sorted slot -> row slot
+  uint16_t* sdig = sidx + TILE;      // digit of each sorted slot
   u32* sexcl = (u32*)(sdig + TILE);  // tile digit counts, then the tile's exclusive prefix
-  u32* sbase = sexcl + RADIX; // global position of the tile's first key of each digit
-  u32* sscan = sbase + RADIX; // 32 words of block-scan scratch
-  u32* sflag = sscan + 32;    // [0] tile id, [1] abort
+  u32* sbase = sexcl + RADIX;        // global position of the tile's first key of each digit
+  u32* sscan = sbase + RADIX;        // 32 words of block-scan scratch
+  u32* sflag = sscan + 32;           // [0] tile id, [1] abort
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
@@ -346,18 +364,35 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   const u32 tile_n = (u32)min((u64)TILE, seg_row1 - base);
   const bool first_tile = tile == seg_tile0;
   const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
+  const bool full = tile_n == (u32)TILE;
   ModelRef model;
   if (a.digit_mode == DIG_MODEL) model = *a.model;
   else model.leaves = nullptr;
 
-  // rd[i]: the item's digit in bits [0, 12) (RADIX = not an item), and after
-  // ranking its rank within the warp in bits [12, 32)
-  // Issue every load of the tile before using any of them (memory-level
-  // parallelism: one DRAM round trip per tile, not one per item).
-  K key[IPT];
-  u32 val[IPT], rd[IPT];
-  const bool full = tile_n == (u32)TILE;
+  // Payload goes straight to shared memory (async copies, no registers),
+  // staged in row order; only the row slot of each sorted position is kept.
   const bool simple_first = FIRST && a.pack.ncols == 1 && a.key_mode == KEY_PACK && !a.gather_idx;
+  if (!FIRST || simple_first) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        const u32 off = warp * 32 * IPT + i * 32 + lane;
+        if (full || off < tile_n) {
+          const u64 idx = base + off;
+          if (!FIRST) cp_async4(spay + w * TILE + off, a.vin[w] + idx);
+          else if (a.pfirst[w].ptr) cp_async4(spay + w * TILE + off, a.pfirst[w].ptr + idx * a.pfirst[w].stride + a.pfirst[w].off);
+          else spay[w * TILE + off] = (u32)idx;
+        }
+      }
+    }
+  }
+
+  // rd[i]: the item's digit in bits [0, 12) (RADIX = not an item), and after
+  // ranking its rank within the warp in bits [12, 32).  Every key load of the
+  // tile is issued before any is used (one DRAM round trip per tile).
+  K key[IPT];
+  u32 rd[IPT];
   if (!FIRST || simple_first) {
     u64 raw[IPT];
 #pragma unroll
@@ -367,8 +402,6 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
       if (full || off < tile_n) {
         if (FIRST) raw[i] = load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, idx);
         else key[i] = ((const K*)a.keys_in)[idx];
-        if (!FIRST) val[i] = a.vals_in[idx];
-        else val[i] = a.vals_first ? a.vals_first[idx] : (u32)idx;
       }
     }
 #pragma unroll
@@ -381,14 +414,23 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
       }
     }
   } else {
+    u64 rows[IPT];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 off = warp * 32 * IPT + i * 32 + lane;
+      const u64 idx = base + off;
+      rows[i] = (off < tile_n && a.gather_idx) ? (u64)a.gather_idx[idx] : idx;
+    }
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
       const u32 off = warp * 32 * IPT + i * 32 + lane;
       if (off < tile_n) {
-        const u64 idx = base + off;
-        const u64 row = a.gather_idx ? (u64)a.gather_idx[idx] : idx;
-        key[i] = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, row) : pack_row<K>(a.pack, row);
-        val[i] = a.vals_first ? a.vals_first[row] : (u32)row;
+        key[i] = a.key_mode == KEY_HASH ? (K)hash_row(a.pack, rows[i]) : pack_row<K>(a.pack, rows[i]);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          if (a.pfirst[w].ptr) cp_async4(spay + w * TILE + off, a.pfirst[w].ptr + rows[i] * a.pfirst[w].stride + a.pfirst[w].off);
+          else spay[w * TILE + off] = (u32)rows[i];
+        }
       }
     }
 #pragma unroll
@@ -462,25 +504,26 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     if (rd[i] & 0x80000000u) {
       const u32 p = rd[i] & 0x1fffu;
       skeys[p] = key[i];
-      svals[p] = val[i];
+      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
       sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
     }
   }
 
   // Resolve each digit's prefix over the earlier tiles and publish it.
-  constexpr int W = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
+  constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sbase[d];
     u32 excl = 0;
     bool bad = false;
     if (!first_tile) {
-      excl = lookback_window<W>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, bad);
+      excl = lookback_window<WIN>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, bad);
       st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
     }
     if (bad) sflag[1] = 1u;
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
     sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
   }
+  cp_async_wait_all();
   __syncthreads();
   if (sflag[1]) return;
 
@@ -488,6 +531,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   for (u32 j = tid; j < tile_n; j += THREADS) {
     const K k = skeys[j];
     const u32 d = sdig[j];
+    const u32 u = sidx[j];
     u64 g = (u64)(u32)(sbase[d] + j);
     if (g < seg_row0 || g >= seg_row1) {  // only reachable if histogram and pass disagree
       atomicOr(a.err, DERR_BOUNDS);
@@ -498,7 +542,8 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     else if (a.segmented && a.seg.key_shift_q)
       kout[g] = (k & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
     else kout[g] = k;
-    a.vals_out[g] = svals[j];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + u];
   }
   if (a.status_next)
     for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
@@ -774,7 +819,8 @@ inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s) {
 // Workspace of one radix sort of n rows (worst case: 64-bit keys).
 struct SortBuffers {
   void* keys[2];   // ping-pong packed keys
-  u32* vals[2];    // ping-pong row ids
+  u32* vals[2][kMaxWords];  // ping-pong payload words (word 0: row ids by default)
+  int words = 1;
   u32* hist;       // [8][2048]
   u32* base;       // [8][2048]
   u32* counters;   // [8]
@@ -791,11 +837,14 @@ inline u64 max_status_words(u64 n) {
   return std::max(std::max(w8, w9), std::max(w10, w11));
 }
 
-inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b) {
+inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b, int words = 1) {
   b.keys[0] = ar.take<u64>(n ? n : 1);
   b.keys[1] = ar.take<u64>(n ? n : 1);
-  b.vals[0] = ar.take<u32>(n ? n : 1);
-  b.vals[1] = ar.take<u32>(n ? n : 1);
+  b.words = words;
+  for (int w = 0; w < kMaxWords; ++w) {
+    b.vals[0][w] = w < words ? ar.take<u32>(n ? n : 1) : nullptr;
+    b.vals[1][w] = w < words ? ar.take<u32>(n ? n : 1) : nullptr;
+  }
   b.hist = ar.take<u32>(8 * 2048);
   b.base = ar.take<u32>(8 * 2048);
   b.counters = ar.take<u32>(64);
@@ -804,18 +853,18 @@ inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b) {
   b.status[1] = ar.take<u32>(b.status_words);
 }
 
-template <typename K, int RB, bool FIRST>
+template <typename K, int RB, bool FIRST, int NW = 1>
 inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles = 0) {
-  using L = PassLayout<K, RB>;
+  using L = PassLayout<K, RB, NW>;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FIRST, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::SMEM));
     attr_set = true;
   }
   int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
   const long t = timing_begin(s);
-  k_onesweep<K, RB, FIRST><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
+  k_onesweep<K, RB, FIRST, NW><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
   if (t >= 0) {
     // algorithmic bytes: the first pass reads the key columns and writes
     // key + row id; later passes read and write key + row id
@@ -824,7 +873,7 @@ inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles 
       for (int j = 0; j < a.pack.ncols; ++j) kraw += dtype_size(a.pack.c[j].dtype);
       if (a.gather_idx) kraw += 4;
     }
-    const double per = FIRST ? kraw + sizeof(K) + 4 : 2.0 * (sizeof(K) + 4);
+    const double per = FIRST ? kraw + sizeof(K) + 4.0 * NW : 2.0 * (sizeof(K) + 4.0 * NW);
     timing_end(t, s, per * (double)n);
   }
   JFX_CUDA(cudaGetLastError());
@@ -841,7 +890,10 @@ struct RadixRequest {
   bool reverse = false;      // descending: write n-1-p in the last pass
   const u32* gather_idx = nullptr;
   u32* targets = nullptr;    // hash partition: digit of each row (row order)
-  u32* perm_out = nullptr;   // sorted row ids
+  u32* perm_out = nullptr;   // sorted row ids (payload word 0 unless vout_final is set)
+  int nwords = 1;            // payload words carried (1..4)
+  PayloadSrc pfirst[kMaxWords] = {};  // first-pass payload sources (null ptr: row id)
+  u32* vout_final[kMaxWords] = {};    // sorted payload words (word 0 defaults to perm_out)
   void* keys_out = nullptr;  // sorted packed keys (K), may be null -> internal buffer
   bool key64 = false;        // packed key type
   void* keys_result = nullptr; // filled: where the sorted packed keys ended up
@@ -855,9 +907,10 @@ struct RadixRequest {
   const ModelRef* model = nullptr;  // DIG_MODEL
 };
 
-template <typename K, int RB>
+template <typename K, int RB, int NW>
 inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
   constexpr int RADIX = 1 << RB;
+  if (NW > b.words) return fail(JFX_ERR_ARG, "sort buffers hold %d payload words, %d requested", b.words, NW);
   int npass;
   int shift[8] = {0}, width[8] = {0};
   if (rq.digit_mode == DIG_MOD) {
@@ -908,16 +961,21 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
   JFX_CUDA(cudaGetLastError());
 
-  u32* out_vals = rq.perm_out;
+  u32* out_vals[kMaxWords];
+  for (int w = 0; w < kMaxWords; ++w) out_vals[w] = rq.vout_final[w];
+  if (!out_vals[0]) out_vals[0] = rq.perm_out;
   void* out_keys = rq.keys_out ? rq.keys_out : b.keys[(npass - 1) & 1];
   for (int p = 0; p < npass; ++p) {
     PassArgs a;
     memset(&a, 0, sizeof a);
     const bool last = p == npass - 1;
     a.keys_in = p ? b.keys[(p - 1) & 1] : nullptr;
-    a.vals_in = p ? b.vals[(p - 1) & 1] : nullptr;
     a.keys_out = last ? out_keys : b.keys[p & 1];
-    a.vals_out = last ? out_vals : b.vals[p & 1];
+    for (int w = 0; w < NW; ++w) {
+      a.vin[w] = p ? b.vals[(p - 1) & 1][w] : nullptr;
+      a.vout[w] = last ? out_vals[w] : b.vals[p & 1][w];
+      a.pfirst[w] = rq.pfirst[w];
+    }
     a.bin_base = b.base + (u64)p * RADIX;
     a.status = b.status[p & 1];
     a.status_next = last ? nullptr : b.status[(p + 1) & 1];
@@ -940,9 +998,9 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     }
     a.pack = rq.pack;
     if (p == 0) {
-      JFX_TRY((launch_pass<K, RB, true>(a, n, s)));
+      JFX_TRY((launch_pass<K, RB, true, NW>(a, n, s)));
     } else {
-      JFX_TRY((launch_pass<K, RB, false>(a, n, s)));
+      JFX_TRY((launch_pass<K, RB, false, NW>(a, n, s)));
     }
   }
   rq.keys_result = out_keys;
@@ -951,6 +1009,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
 
 template <typename K>
 inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
+  if (rq.nwords > 1 && rq.digit_mode == DIG_BITS) rq.max_digit_bits = 8;
   int rb;
   if (rq.digit_mode == DIG_MOD) {
     rb = rq.modulus <= 256 ? 8 : rq.modulus <= 512 ? 9 : rq.modulus <= 1024 ? 10 : 11;
@@ -959,11 +1018,20 @@ inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaSt
     int w = ceil_div(rq.total_bits, npass);
     rb = w <= 8 ? 8 : w;
   }
+  if (rq.nwords > 1) {  // payload-carrying sorts use 8-bit digits
+    if (rq.digit_mode == DIG_BITS) rq.max_digit_bits = 8;
+    switch (rq.nwords) {
+      case 2: return run_radix<K, 8, 2>(rq, n, b, err, s);
+      case 3: return run_radix<K, 8, 3>(rq, n, b, err, s);
+      case 4: return run_radix<K, 8, 4>(rq, n, b, err, s);
+    }
+    return fail(JFX_ERR_ARG, "1..4 payload words supported");
+  }
   switch (rb) {
-    case 8: return run_radix<K, 8>(rq, n, b, err, s);
-    case 9: return run_radix<K, 9>(rq, n, b, err, s);
-    case 10: return run_radix<K, 10>(rq, n, b, err, s);
-    case 11: return run_radix<K, 11>(rq, n, b, err, s);
+    case 8: return run_radix<K, 8, 1>(rq, n, b, err, s);
+    case 9: return run_radix<K, 9, 1>(rq, n, b, err, s);
+    case 10: return run_radix<K, 10, 1>(rq, n, b, err, s);
+    case 11: return run_radix<K, 11, 1>(rq, n, b, err, s);
   }
   return fail(JFX_ERR_ARG, "digit width %d unsupported", rb);
 }
@@ -974,6 +1042,8 @@ inline int radix_sort(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStr
   if (n > (u64)kMaxRows) return fail(JFX_ERR_CAPACITY, "%llu rows exceed the %lld-row limit", n, (long long)kMaxRows);
   if (rq.digit_mode == DIG_BITS && rq.total_bits == 0) {
     int grid = (int)std::min<u64>((n + 255) / 256, 4096);
+    if (rq.nwords > 1 || rq.pfirst[0].ptr || rq.reverse && rq.nwords > 1)
+      return fail(JFX_ERR_ARG, "constant keys with a payload: carry it with total_bits >= 1");
     k_iota<<<std::max(grid, 1), 256, 0, s>>>(rq.perm_out, n, rq.reverse ? 1 : 0), note_launch();
     void* out_keys = rq.keys_out ? rq.keys_out : b.keys[0];
     if (rq.key64) k_fill_keys<u64><<<std::max(grid, 1), 256, 0, s>>>((u64*)out_keys, n), note_launch();
