@@ -187,6 +187,7 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
 
 // ---------------------------------------------------------------- learned ---
 struct LearnedBuffers {
+  u32* spos;  // predicted position of each key, in sorted order
   u64* sample;
   u64* ssorted;
   u32* sperm;
@@ -201,7 +202,9 @@ struct LearnedBuffers {
   u64 s, tiles;
 };
 static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBuffers& l) {
-  carve_sort(ar, n, c, b);
+  take_common(ar, c);
+  take_sort_buffers(ar, n, b, 3);
+  l.spos = ar.take<u32>(n ? n : 1);
   l.s = n / kSampleStride;
   l.sample = ar.take<u64>(l.s + 1);
   l.ssorted = ar.take<u64>(l.s + 1);
@@ -1009,23 +1012,31 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   const u64 npos = 4 * N;
   k_leaf_finalize<<<1, 1024, 0, s>>>(l.ssorted, l.s, npos, l.first, l.last, l.fit, l.leaves, l.flags), note_launch();
   JFX_CUDA(cudaGetLastError());
-  // 3. radix passes over the predicted position
+  // 3. radix passes over the predicted position: the first pass evaluates the
+  // model once per key and sorts by the position, carrying the key (two
+  // words) and the row id; the last pass writes the key as one u64
   {
     jfx_column col{keys, JFX_U64, 0u};
     RadixRequest rq;
     JFX_TRY(build_pack(&col, 1, 0u, false, rq.pack));
     rq.pack.c[0].bits = 64;
-    rq.digit_mode = DIG_MODEL;
+    rq.key_mode = KEY_MODEL;
+    rq.digit_mode = DIG_BITS;
     rq.model = l.model;
     rq.total_bits = std::max(1, bit_length(npos - 1));
-    rq.key64 = true;
-    rq.perm_out = (u32*)perm_out;
-    rq.keys_out = sorted_keys_out;
+    rq.key64 = false;
+    rq.nwords = 3;
+    rq.pfirst[0] = PayloadSrc{(const unsigned char*)keys, 8u, 0u};
+    rq.pfirst[1] = PayloadSrc{(const unsigned char*)keys, 8u, 4u};
+    rq.pfirst[2] = PayloadSrc{nullptr, 0u, 0u};
+    rq.vout64 = sorted_keys_out;
+    rq.vout_final[2] = (u32*)perm_out;
+    rq.keys_out = l.spos;
     JFX_TRY(radix_sort(rq, N, b, c.err, s));
   }
   // 4. fix-up of runs of equal predicted position
   JFX_CUDA(cudaMemsetAsync(l.fix.counts, 0, 8 * sizeof(u32), s));
-  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, N, l.model, l.fix), note_launch();
+  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.spos, N, l.fix), note_launch();
   k_fix_check<<<grid_for(l.tiles, 256), 256, 0, s>>>(l.tiles, l.fix), note_launch();
   k_fix_small<<<device_sm_count() * 8, 256, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
   {

@@ -211,22 +211,20 @@ __device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
 
 // Lists the runs of equal predicted position that start in this CTA's tile
 // and contain an inversion.
-__global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals, u64 n, const ModelRef* mp,
+__global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals, const u32* spos, u64 n,
                                                            FixLists L) {
   __shared__ u64 sk[kFindTile + 1];
   __shared__ u32 sp[kFindTile + 1];
   __shared__ u32 sv[kFindTile + 1];
   __shared__ u32 fb[kFindTile / 32 + 2], ib[kFindTile / 32 + 2];
   __shared__ int s_open;
-  const ModelRef m = *mp;
   const u64 t0 = (u64)blockIdx.x * kFindTile;
   const u64 t1 = min(n, t0 + kFindTile);
   const u64 base = t0 ? t0 - 1 : 0;
   const u32 len = (u32)(t1 - base);  // window: [base, t1)
   for (u32 i = threadIdx.x; i < len; i += kFindThreads) {
-    const u64 k = keys[base + i];
-    sk[i] = k;
-    sp[i] = model_pos(m, k);
+    sk[i] = keys[base + i];
+    sp[i] = spos[base + i];
   }
   if (threadIdx.x == 0) s_open = -1;
   __syncthreads();
@@ -338,7 +336,7 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
     const u64 q = pos + lane;
     const bool in = q < n;
     const u64 k = in ? keys[q] : 0;
-    const bool same = in && model_pos(m, k) == p0;
+    const bool same = in && spos[q] == p0;
     const u32 bs = __ballot_sync(0xffffffffu, same);
     const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
     const u64 km = lane == 0 ? prev_key : kp;

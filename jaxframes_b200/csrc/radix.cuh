@@ -65,6 +65,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 enum : int {
   KEY_PACK = 0,   // first pass packs the key columns (pack_row)
   KEY_HASH = 1,   // first pass hashes the key columns (hash_multi_columns)
+  KEY_MODEL = 2,  // first pass: key = learned-model position of the uint64 key column
   DIG_BITS = 0,   // digit = (key >> shift) & mask
   DIG_MOD = 1,    // digit = key % modulus (hash partition)
   DIG_MODEL = 2,  // digit = (model position of key >> shift) & mask (learned sort)
@@ -146,7 +147,8 @@ struct PassArgs {
   int raw_dtype;
   u32 raw_flags;
   u64 raw_tmin;
-  const ModelRef* model; // DIG_MODEL: device-resident model
+  const ModelRef* model; // DIG_MODEL / KEY_MODEL: device-resident model
+  unsigned long long* vout64;  // last pass: payload words 0 and 1 written as one u64 here
   int segmented;
   SegTables seg;
   PackDesc pack;
@@ -324,6 +326,15 @@ __device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 
   }
 }
 
+// Packed key of two columns from their raw elements.
+template <typename K>
+__device__ __forceinline__ K pack2(const PackDesc& pd, u64 r0, u64 r1) {
+  K k = 0;
+  if (pd.c[0].bits) k |= (K)((transform_raw(pd.c[0], r0) - pd.c[0].tmin) << pd.c[0].shift);
+  if (pd.c[1].bits) k |= (K)((transform_raw(pd.c[1], r1) - pd.c[1].tmin) << pd.c[1].shift);
+  return k;
+}
+
 template <typename K, int RB, bool FIRST, int NW>
 __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
   using L = PassLayout<K, RB, NW>;
@@ -366,12 +377,14 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
   const bool full = tile_n == (u32)TILE;
   ModelRef model;
-  if (a.digit_mode == DIG_MODEL) model = *a.model;
+  if (a.digit_mode == DIG_MODEL || (FIRST && a.key_mode == KEY_MODEL)) model = *a.model;
   else model.leaves = nullptr;
 
   // Payload goes straight to shared memory (async copies, no registers),
   // staged in row order; only the row slot of each sorted position is kept.
-  const bool simple_first = FIRST && a.pack.ncols == 1 && a.key_mode == KEY_PACK && !a.gather_idx;
+  const bool two_first = FIRST && a.pack.ncols == 2 && a.key_mode == KEY_PACK && !a.gather_idx;
+  const bool simple_first = FIRST && (a.pack.ncols == 1 || two_first) &&
+                            (a.key_mode == KEY_PACK || a.key_mode == KEY_MODEL) && !a.gather_idx;
   if (!FIRST || simple_first) {
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
@@ -393,7 +406,31 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   // tile is issued before any is used (one DRAM round trip per tile).
   K key[IPT];
   u32 rd[IPT];
-  if (!FIRST || simple_first) {
+  if (two_first) {
+    // two key columns: both columns' loads for 8 items, then pack
+#pragma unroll
+    for (int i0 = 0; i0 < IPT; i0 += 8) {
+      u64 r0[8], r1[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const u32 off = warp * 32 * IPT + (i0 + i) * 32 + lane;
+        const u64 idx = base + off;
+        if (full || off < tile_n) {
+          r0[i] = load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, idx);
+          r1[i] = load_raw(a.pack.c[1].ptr, a.pack.c[1].dtype, idx);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const u32 off = warp * 32 * IPT + (i0 + i) * 32 + lane;
+        rd[i0 + i] = RADIX;
+        if (full || off < tile_n) {
+          key[i0 + i] = pack2<K>(a.pack, r0[i], r1[i]);
+          rd[i0 + i] = digit_of<K>(key[i0 + i], a.digit_mode, a.shift, mask, a.modulus, model);
+        }
+      }
+    }
+  } else if (!FIRST || (simple_first && a.pack.ncols == 1)) {
     u64 raw[IPT];
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
@@ -409,7 +446,10 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
       const u32 off = warp * 32 * IPT + i * 32 + lane;
       rd[i] = RADIX;
       if (full || off < tile_n) {
-        if (FIRST) key[i] = (K)(transform_raw(a.pack.c[0], raw[i]) - a.pack.c[0].tmin) << a.pack.c[0].shift;
+        if (FIRST) {
+          const u64 t = transform_raw(a.pack.c[0], raw[i]);
+          key[i] = a.key_mode == KEY_MODEL ? (K)model_pos(model, t) : (K)(t - a.pack.c[0].tmin) << a.pack.c[0].shift;
+        }
         rd[i] = digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model);
       }
     }
@@ -498,19 +538,10 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
                 ? 0x80000000u | (d << 13) | (sexcl[d] + (u32)whist[warp * RADIX + d] + (rd[i] >> 12))
                 : 0u;
   }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    if (rd[i] & 0x80000000u) {
-      const u32 p = rd[i] & 0x1fffu;
-      skeys[p] = key[i];
-      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
-      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
-    }
-  }
 
-  // Resolve each digit's prefix over the earlier tiles and publish it.
-  constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
+  // Resolve each digit's prefix over the earlier tiles and publish it as
+  // early as possible (successors walk back until an inclusive word).
+  constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 32;
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sbase[d];
     u32 excl = 0;
@@ -523,11 +554,57 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
     sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
   }
+  __syncthreads();  // whist reads above are done before skeys (aliased) is written
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    if (rd[i] & 0x80000000u) {
+      const u32 p = rd[i] & 0x1fffu;
+      skeys[p] = key[i];
+      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
+      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
+    }
+  }
   cp_async_wait_all();
   __syncthreads();
   if (sflag[1]) return;
 
   K* kout = (K*)a.keys_out;
+  const bool plain_out = !a.raw_out && !a.reverse && !(a.segmented && a.seg.key_shift_q);
+  if (full && plain_out) {
+    // full tile: IPT independent slots per thread, loads before stores
+#pragma unroll
+    for (int i0 = 0; i0 < IPT; i0 += 8) {
+      K kk[8];
+      u32 gg[8], uu[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const u32 j = (i0 + i) * THREADS + tid;
+        kk[i] = skeys[j];
+        uu[i] = sidx[j];
+        gg[i] = sbase[sdig[j]] + j;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const u64 g = gg[i];
+        if (g < seg_row0 || g >= seg_row1) {
+          atomicOr(a.err, DERR_BOUNDS);
+          continue;
+        }
+        kout[g] = kk[i];
+        if (NW >= 2 && a.vout64) {
+          a.vout64[g] = (unsigned long long)spay[uu[i]] | ((unsigned long long)spay[TILE + uu[i]] << 32);
+#pragma unroll
+          for (int w = 2; w < NW; ++w) a.vout[w][g] = spay[w * TILE + uu[i]];
+        } else {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + uu[i]];
+        }
+      }
+    }
+    if (a.status_next)
+      for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
+    return;
+  }
   for (u32 j = tid; j < tile_n; j += THREADS) {
     const K k = skeys[j];
     const u32 d = sdig[j];
@@ -542,8 +619,14 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     else if (a.segmented && a.seg.key_shift_q)
       kout[g] = (k & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
     else kout[g] = k;
+    if (NW >= 2 && a.vout64) {
+      a.vout64[g] = (unsigned long long)spay[u] | ((unsigned long long)spay[TILE + u] << 32);
 #pragma unroll
-    for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + u];
+      for (int w = 2; w < NW; ++w) a.vout[w][g] = spay[w * TILE + u];
+    } else {
+#pragma unroll
+      for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + u];
+    }
   }
   if (a.status_next)
     for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
@@ -574,14 +657,23 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
 #pragma unroll
   for (int p = 0; p < 8; ++p) mask[p] = a.width[p] >= 32 ? 0xffffffffu : ((1u << a.width[p]) - 1u);
   ModelRef model;
-  if (a.digit_mode == DIG_MODEL) model = *a.model;
+  if (a.digit_mode == DIG_MODEL || a.key_mode == KEY_MODEL) model = *a.model;
   else model.leaves = nullptr;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   constexpr int U = 8;  // rows per thread per step, loads issued together
   const bool simple = a.pack.ncols == 1 && a.key_mode == KEY_PACK;
   for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < a.n; r0 += stride * U) {
     K kk[U];
-    if (simple) {
+    if (a.key_mode == KEY_MODEL) {
+      u64 raw[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        raw[u] = r < a.n ? load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, r) : 0ull;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) kk[u] = (K)model_pos(model, transform_raw(a.pack.c[0], raw[u]));
+    } else if (simple) {
       u64 raw[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -591,6 +683,16 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
 #pragma unroll
       for (int u = 0; u < U; ++u)
         kk[u] = (K)(transform_raw(a.pack.c[0], raw[u]) - a.pack.c[0].tmin) << a.pack.c[0].shift;
+    } else if (a.pack.ncols == 2 && a.key_mode == KEY_PACK) {
+      u64 x0[U], x1[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 r = r0 + (u64)u * stride;
+        x0[u] = r < a.n ? load_raw(a.pack.c[0].ptr, a.pack.c[0].dtype, r) : 0ull;
+        x1[u] = r < a.n ? load_raw(a.pack.c[1].ptr, a.pack.c[1].dtype, r) : 0ull;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) kk[u] = pack2<K>(a.pack, x0[u], x1[u]);
     } else {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -904,7 +1006,8 @@ struct RadixRequest {
   int raw_dtype = 0;
   u32 raw_flags = 0;
   u64 raw_tmin = 0;
-  const ModelRef* model = nullptr;  // DIG_MODEL
+  const ModelRef* model = nullptr;  // DIG_MODEL / KEY_MODEL
+  unsigned long long* vout64 = nullptr;  // last pass: words 0 and 1 as one u64
 };
 
 template <typename K, int RB, int NW>
@@ -989,6 +1092,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     a.digit_mode = rq.digit_mode;
     a.modulus = rq.modulus;
     a.model = rq.model;
+    a.vout64 = last ? rq.vout64 : nullptr;
     a.reverse = last && rq.reverse;
     if (last && rq.raw_out) {
       a.raw_out = rq.raw_out;
