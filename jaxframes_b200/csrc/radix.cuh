@@ -525,8 +525,6 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     sbase[d] = c;
     st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | c);
   }
-  // Tile-local exclusive prefix and shared-memory sort by digit come before
-  // the look-back, which gives earlier tiles time to publish inclusive sums.
   block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);
 
   static_assert(TILE <= 8192 && RADIX <= 2048, "position/digit packing");
@@ -538,10 +536,21 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
                 ? 0x80000000u | (d << 13) | (sexcl[d] + (u32)whist[warp * RADIX + d] + (rd[i] >> 12))
                 : 0u;
   }
+  __syncthreads();  // whist reads above are done before skeys (aliased) is written
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    if (rd[i] & 0x80000000u) {
+      const u32 p = rd[i] & 0x1fffu;
+      skeys[p] = key[i];
+      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
+      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
+    }
+  }
 
-  // Resolve each digit's prefix over the earlier tiles and publish it as
-  // early as possible (successors walk back until an inclusive word).
-  constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 32;
+  // Resolve each digit's prefix over the earlier tiles and publish it.  The
+  // local sort above comes first: it gives earlier tiles time to publish, so
+  // the walk back rarely has to wait.
+  constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sbase[d];
     u32 excl = 0;
@@ -553,16 +562,6 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     if (bad) sflag[1] = 1u;
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
     sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
-  }
-  __syncthreads();  // whist reads above are done before skeys (aliased) is written
-#pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    if (rd[i] & 0x80000000u) {
-      const u32 p = rd[i] & 0x1fffu;
-      skeys[p] = key[i];
-      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
-      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
-    }
   }
   cp_async_wait_all();
   __syncthreads();
