@@ -97,6 +97,21 @@ size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2);
 int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
              void* sorted_keys_out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* jfx_sort without a workspace, for callers that cannot allocate device
+ * memory (inside an allocator or memory-pool callback, in loops that must not
+ * take cudaMalloc's device-wide synchronisation, or as a plugin that is
+ * handed only its input and output buffers).  No counterpart in the
+ * reference.  Same arguments, results and errors as jfx_sort; the scratch is a
+ * fixed 16 MiB device array inside the library, so n is limited to
+ * JFX_SORT_STATIC_MAX_ROWS (JFX_ERR_CAPACITY beyond it).  Allocates nothing:
+ * no cudaMalloc / cudaFree and no pinned host memory.  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller. */
+#define JFX_SORT_STATIC_MAX_ROWS 524288
+int jfx_sort_static(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
+                    void* sorted_keys_out, void* stream);
+
 /* multi_column_lexsort (parallel_algorithms.py:25-66): stable lexicographic
  * argsort of ncols columns (first column most significant), JFX_COL_DESC per
  * column.  One column: ascending ignored, as in the reference. */

@@ -34,6 +34,7 @@ AGG_SUM, AGG_MEAN, AGG_COUNT, AGG_MIN, AGG_MAX = 1, 2, 4, 8, 16
 AGG_BITS = {"sum": AGG_SUM, "mean": AGG_MEAN, "count": AGG_COUNT, "min": AGG_MIN, "max": AGG_MAX}
 JOIN_KINDS = {"inner": 0, "left": 1, "right": 2, "outer": 3}
 WS_SORT, WS_GROUPBY, WS_JOIN, WS_PARTITION, WS_LEARNED, WS_BATCH = 1, 2, 3, 4, 5, 6
+SORT_STATIC_MAX_ROWS = 524288  # JFX_SORT_STATIC_MAX_ROWS
 
 
 class JfxUnavailable(RuntimeError):
@@ -79,6 +80,7 @@ SIGNATURES = {
     "jfx_max_rows": (_INT, []),
     "jfx_workspace_size": (_SIZE, [_INT, _I64, _I64]),
     "jfx_sort": (_INT, [ctypes.POINTER(Column), _I64, _INT, _P, _P, _P, _SIZE, _P]),
+    "jfx_sort_static": (_INT, [ctypes.POINTER(Column), _I64, _INT, _P, _P, _P]),
     "jfx_lexsort": (_INT, [ctypes.POINTER(Column), _INT, _I64, _P, _P, _SIZE, _P]),
     "jfx_groupby": (_INT, [ctypes.POINTER(Column), _INT, _I64, _INT, ctypes.POINTER(AggColumn), _INT,
                            ctypes.POINTER(_P), ctypes.POINTER(_I64), _P, _SIZE, _P]),

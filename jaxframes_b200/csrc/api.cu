@@ -317,6 +317,40 @@ static int check_n(int64_t n) {
   return JFX_OK;
 }
 
+
+// ------------------------------------------------ sort without allocation ---
+// Scratch of jfx_sort_static: a fixed device array in this library instead of
+// a caller workspace.  Every device that loads the library holds it until the
+// process exits.  It is sized for the sort buffers of kStaticSortMaxRows rows
+// (64-bit keys, the widest digit configuration); jfx_sort_static checks that
+// the carve fits before it launches anything.
+constexpr int64_t kStaticSortMaxRows = JFX_SORT_STATIC_MAX_ROWS;
+constexpr size_t kStaticSortScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_static_sort_scratch[kStaticSortScratchBytes];
+
+// Device address of g_static_sort_scratch on the current device.  In host
+// code the array's name is only a host-side stand-in for the symbol, so the
+// address is looked up once per device (with that device current) and
+// cached; the lookup may load this library's device code on that device.
+static int static_sort_scratch(void** out) {
+  static std::mutex mu;
+  static void* addr[128] = {nullptr};
+  int dev = -1;
+  JFX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(JFX_ERR_ARG, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_sort_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(JFX_ERR_CUDA, "cudaGetSymbolAddress of the static sort scratch failed on device %d: %s", dev,
+                  cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return JFX_OK;
+}
+
 }  // namespace jfx
 
 using namespace jfx;
@@ -457,6 +491,74 @@ int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
     JFX_CUDA(cudaGetLastError());
   }
   u64* host = g_host.get();
+  JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+  return check_err_word((u32)host[0]);
+}
+
+// jfx_sort without a workspace argument: the scratch is g_static_sort_scratch.
+// Callers that cannot allocate device memory use it: code that runs inside a
+// memory-pool or allocator callback (allocating there would re-enter the
+// allocator), loops that must not take cudaMalloc's implicit device-wide
+// synchronisation, and host frameworks that own all device memory and hand a
+// plugin only its input and output buffers.  Nothing here allocates: no
+// cudaMalloc / cudaFree, no pinned host buffer (read-backs go to the stack),
+// no library allocator.  The first call on a device looks up the scratch
+// address (static_sort_scratch), so make it before any stream capture.  Every
+// call shares the one array and finds the previous call's data there: the
+// error word, the digit histograms, the tile counter and the first pass's
+// look-back words are cleared on the stream before use (the rest is written
+// before it is read).  Calls whose work overlaps on the GPU -- two streams, or
+// two host threads -- race on the array and must be serialised by the caller.
+int jfx_sort_static(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out, void* sorted_keys_out,
+                    void* stream) {
+  JFX_TRY(check_n(n));
+  if (n > kStaticSortMaxRows)
+    return fail(JFX_ERR_CAPACITY, "jfx_sort_static takes at most %lld rows (got %lld): its scratch is a fixed "
+                "%zu-byte device array; use jfx_sort with a workspace for more", (long long)kStaticSortMaxRows,
+                (long long)n, kStaticSortScratchBytes);
+  if (!key || !perm_out) return fail(JFX_ERR_ARG, "null key or permutation pointer");
+  if (n == 0) return JFX_OK;
+  cudaStream_t s = as_stream(stream);
+  PackDesc pd;
+  JFX_TRY(build_pack(key, 1, CF_QUIRK, false, pd));
+  if (key->dtype == JFX_BOOL) return fail(JFX_ERR_DTYPE, "ParallelRadixSort cannot shift a bool key");
+  void* scratch = nullptr;
+  JFX_TRY(static_sort_scratch(&scratch));
+  Arena ar(scratch, kStaticSortScratchBytes);
+  Common c;
+  SortBuffers b;
+  carve_sort(ar, (u64)n, c, b);
+  if (ar.overflow) return fail(JFX_ERR_ALLOC, "static sort scratch of %zu bytes < %zu needed", kStaticSortScratchBytes, ar.off);
+  u64 host[2 * kMaxCols];  // read-back words (pageable: no pinned buffer is allocated)
+  JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
+  KeyPlan kp;
+  kp.pack = pd;
+  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s, host));
+  RadixRequest rq;
+  rq.pack = kp.pack;
+  rq.total_bits = kp.total_bits;
+  rq.key64 = kp.total_bits > 32;
+  rq.reverse = !ascending;
+  rq.perm_out = (u32*)perm_out;
+  const bool int_keys = !dtype_is_float(key->dtype);
+  if (sorted_keys_out && int_keys && kp.total_bits > 0) {
+    rq.raw_out = sorted_keys_out;
+    rq.raw_dtype = key->dtype;
+    rq.raw_flags = CF_QUIRK;
+    rq.raw_tmin = kp.pack.c[0].tmin;
+  }
+  JFX_TRY(radix_sort(rq, (u64)n, b, c.err, s));
+  if (sorted_keys_out && !(int_keys && kp.total_bits > 0)) {
+    const int g = grid_for((u64)n, 256);
+    if (dtype_is_float(key->dtype)) {
+      k_gather_same<<<g, 256, 0, s>>>(key->data, key->dtype, (const u32*)perm_out, (u64)n, sorted_keys_out), note_launch();
+    } else if (rq.key64) {
+      k_unpack<u64><<<g, 256, 0, s>>>((const u64*)rq.keys_result, (u64)n, key->dtype, CF_QUIRK, kp.pack.c[0].tmin, sorted_keys_out), note_launch();
+    } else {
+      k_unpack<u32><<<g, 256, 0, s>>>((const u32*)rq.keys_result, (u64)n, key->dtype, CF_QUIRK, kp.pack.c[0].tmin, sorted_keys_out), note_launch();
+    }
+    JFX_CUDA(cudaGetLastError());
+  }
   JFX_TRY(read_back(c.err, sizeof(u32), host, s));
   return check_err_word((u32)host[0]);
 }

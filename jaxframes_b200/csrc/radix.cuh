@@ -878,9 +878,11 @@ inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s
 // Computes min/max of every key column (two reductions when an integer column
 // is descending: max(x) first, then the rewritten values) and assigns the bit
 // fields.  One stream synchronisation.
-inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s) {
+// host: 2 * ncols words of host memory for the read-back (null: the pinned
+// per-thread buffer).
+inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s, u64* host = nullptr) {
   PackDesc& pd = kp.pack;
-  u64* host = g_host.get();
+  if (!host) host = g_host.get();
   if (!host) return fail(JFX_ERR_CUDA, "cudaMallocHost failed");
   bool need_raw_max = false;
   for (int j = 0; j < pd.ncols; ++j)
