@@ -380,6 +380,9 @@ def run_secondary(args):
     b.build()
     import jaxframes_b200.parallel_algorithms as P
     dev = torch.device("cuda", 0)
+    if args.workload == "batch":
+        run_batch(args, dev)
+        return
     if args.workload == "groupby":
         n = args.n or 100_000_000
         k1, k2, v1, v2 = [torch.from_numpy(x).to(dev) for x in c3_inputs(n)]
@@ -435,6 +438,49 @@ def run_secondary(args):
     ms = a.elapsed_time(b2) / args.steps
     print(json.dumps({"workload": args.workload, "rows": n, "ms_per_step": ms, "rows_per_s": unit_rows / (ms / 1e3)}),
           flush=True)
+
+
+def run_batch(args, dev):
+    """Batched hash partition (256 partitions) + groupby-sum over 2048 queries
+    with row counts floor(exp(uniform(ln 1e3, ln 4e6))) (about 1e9 rows),
+    int32 keys uniform in [0, min(rows // 4, 1e6)), float32 N(0, 1) values;
+    one CUDA-graph replay per step.  Inputs are generated on the device from a
+    seeded generator."""
+    import torch
+    from jaxframes_b200.batch import BatchedGroupBy
+    nq = 2048
+    rng = np.random.default_rng(46)
+    rows = np.floor(np.exp(rng.uniform(np.log(1e3), np.log(4e6), nq))).astype(np.int64)
+    if args.n:  # scaled-down batch with the same shape of row counts
+        rows = np.maximum(1, np.floor(rows * (args.n / rows.sum()))).astype(np.int64)
+    off = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    n = int(off[-1])
+    b = BatchedGroupBy(n, nq, 256, 20, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(46)
+    for q in range(nq):
+        span = int(max(1, min(rows[q] // 4, 1_000_000)))
+        b.keys[off[q]:off[q + 1]] = torch.randint(0, span, (int(rows[q]),), generator=g, device=dev,
+                                                  dtype=torch.int32)
+    torch.randn(n, generator=g, device=dev, out=b.values[:n])
+    b.query_offsets.copy_(torch.from_numpy(off))
+    b.capture()
+    for _ in range(args.warmup):
+        b.replay()
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        b.replay()
+    e.record()
+    torch.cuda.synchronize()
+    b.status()
+    ms = a.elapsed_time(e) / args.steps
+    groups = int(b.group_offsets[nq].item())
+    model = 56 * n + 8 * groups  # partition 16 + sort 28 + groupby 12 bytes per row, 8 per group
+    print(json.dumps({"workload": "batch", "queries": nq, "rows": n, "groups": groups, "ms_per_step": ms,
+                      "rows_per_s": n / (ms / 1e3), "model_gbs": model / (ms / 1e3) / 1e9,
+                      "graph": "one CUDA graph replay per step"}), flush=True)
 
 
 def run_extra(args, P, dev):
@@ -501,7 +547,7 @@ def main():
     ap.add_argument("--impl", default="jfx", choices=["jfx", "reference"])
     ap.add_argument("--extra", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", default="join", choices=["join", "groupby", "sort", "groupby1m", "learned"],
+    ap.add_argument("--workload", default="join", choices=["join", "groupby", "sort", "groupby1m", "learned", "batch"],
                     help="join = the headline; the others time one secondary config alone")
     ap.add_argument("--n", type=int, default=0, help="rows for --workload groupby/sort (0 = config size)")
     ap.add_argument("--profile", action="store_true", help="timed steps only (no e2e, CPU leg or extras)")

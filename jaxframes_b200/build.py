@@ -24,6 +24,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr",
     "-Xcudafe", "--diag_suppress=177",
+    "-split-compile=0",  # optimise the kernels in parallel, one job per host core
 ]
 
 

@@ -38,7 +38,7 @@ template <typename K, int RB, int NW = 1>
 struct PassLayout {
   static constexpr int THREADS = RadixCfg<RB>::THREADS, IPT = RadixCfg<RB>::IPT;
   static constexpr int RADIX = 1 << RB, WARPS = THREADS / 32, TILE = THREADS * IPT;
-  static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 2;
+  static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 4;
   static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
   static constexpr size_t A_BYTES = HIST_BYTES > KEY_BYTES ? HIST_BYTES : KEY_BYTES;
   static constexpr size_t PAY_BYTES = (size_t)NW * TILE * 4;  // payload staged in row order
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   constexpr int THREADS = L::THREADS, IPT = L::IPT, RADIX = L::RADIX, WARPS = L::WARPS,
                 TILE = L::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
-  uint16_t* whist = (uint16_t*)smem;  // [WARPS][RADIX] during ranking
+  u32* whist = (u32*)smem;  // [WARPS][RADIX] during ranking
   K* skeys = (K*)smem;                // [TILE] after ranking (aliases whist)
   u32* spay = (u32*)(smem + L::A_BYTES);                 // [NW][TILE] payload, row order
   uint16_t* sidx = (uint16_t*)(smem + L::A_BYTES + L::PAY_BYTES);  // sorted slot -> row slot
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     sflag[0] = atomicAdd(a.tile_counter, 1u);
     sflag[1] = 0;
   }
-  for (int i = tid; i < WARPS * RADIX / 2; i += THREADS) ((u32*)whist)[i] = 0u;
+  for (int i = tid; i < WARPS * RADIX; i += THREADS) whist[i] = 0u;
   __syncthreads();
   const u32 tile = sflag[0];
   // segment of the tile: rows [seg_row0, seg_row1), tiles from seg_tile0
@@ -385,12 +385,23 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   const bool two_first = FIRST && a.pack.ncols == 2 && a.key_mode == KEY_PACK && !a.gather_idx;
   const bool simple_first = FIRST && (a.pack.ncols == 1 || two_first) &&
                             (a.key_mode == KEY_PACK || a.key_mode == KEY_MODEL) && !a.gather_idx;
-  if (!FIRST || simple_first) {
+  // this thread's first slot in the tile; item i sits at toff + 32 i
+  const u32 toff = warp * 32 * IPT + lane;
+  if (!FIRST && full) {
+    // later pass, full tile: per-thread base pointers, immediate offsets
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      const u32* src = a.vin[w] + base + toff;
+      u32* dst = spay + w * TILE + toff;
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) cp_async4(dst + i * 32, src + i * 32);
+    }
+  } else if (!FIRST || simple_first) {
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
-        const u32 off = warp * 32 * IPT + i * 32 + lane;
+        const u32 off = toff + i * 32;
         if (full || off < tile_n) {
           const u64 idx = base + off;
           if (!FIRST) cp_async4(spay + w * TILE + off, a.vin[w] + idx);
@@ -406,7 +417,39 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   // tile is issued before any is used (one DRAM round trip per tile).
   K key[IPT];
   u32 rd[IPT];
-  if (two_first) {
+  // first pass over one plain 32/64-bit integer column (the common key):
+  // the dtype dispatch happens once per tile, not per item
+  const int d0 = a.pack.c[0].dtype;
+  const bool int_first = FIRST && full && simple_first && a.pack.ncols == 1 && a.key_mode == KEY_PACK &&
+                         a.digit_mode == DIG_BITS && !(a.pack.c[0].flags & CF_DESC) &&
+                         (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
+  if (!FIRST && full && a.digit_mode == DIG_BITS) {
+    const K* kin = (const K*)a.keys_in + base + toff;
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) key[i] = kin[i * 32];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) rd[i] = (u32)(key[i] >> a.shift) & mask;
+  } else if (int_first) {
+    u64 raw[IPT];
+    if (d0 == JFX_I64 || d0 == JFX_U64) {
+      const u64* src = (const u64*)a.pack.c[0].ptr + base + toff;
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) raw[i] = __ldg(src + i * 32);
+    } else {
+      const u32* src = (const u32*)a.pack.c[0].ptr + base + toff;
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) raw[i] = __ldg(src + i * 32);
+    }
+    // order-preserving transform of transform_raw for these types: flip the sign bit
+    const u64 flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
+    const u64 tmin = a.pack.c[0].tmin;
+    const int kshift = a.pack.c[0].shift;
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      key[i] = (K)(((raw[i] ^ flip) - tmin) << kshift);
+      rd[i] = (u32)(key[i] >> a.shift) & mask;
+    }
+  } else if (two_first) {
     // two key columns: both columns' loads for 8 items, then pack
 #pragma unroll
     for (int i0 = 0; i0 < IPT; i0 += 8) {
@@ -480,76 +523,35 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     }
   }
 
-  // Stable rank within the warp: lanes holding the same digit are ranked by
-  // lane, and items are visited in row order, so equal digits keep row order.
-  // Peers are found with one ballot per digit bit.
-  const u32 lt = lanemask_lt(), gt = lanemask_gt();
-  uint16_t* wh = whist + warp * RADIX;
+  // Digit counts first: per-warp histograms by shared-memory atomics (order
+  // does not matter for a count), so the tile's counts are published and its
+  // prefix over earlier tiles resolved before the ranking, which is the
+  // longest phase.  Successors then find this tile's words early.
+  u32* wh = whist + warp * RADIX;
 #pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    const u32 d = rd[i];
-    const bool valid = d < (u32)RADIX;
-    u32 peers = __ballot_sync(0xffffffffu, valid);
-    if (!valid) peers = ~peers;
-#pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const u32 bit = (d >> b) & 1u;
-      const u32 bb = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? bb : ~bb;
-    }
-    const u32 prior = valid ? (u32)wh[d] : 0u;
-    rd[i] = d | ((prior + __popc(peers & lt)) << 12);
-    __syncwarp();
-    if (valid && !(peers & gt)) wh[d] = (uint16_t)(prior + __popc(peers));
-    __syncwarp();
-  }
+  for (int i = 0; i < IPT; ++i)
+    if (rd[i] < (u32)RADIX) atomicAdd(&wh[rd[i]], 1u);
   __syncthreads();
 
-  // Per digit: exclusive prefix over warps (in place) and the tile count.
+  // Per digit: exclusive prefix over warps (in place), the tile count, and
+  // its publication (tile 0 of a segment: already inclusive).
+  u32* st = a.status + (u64)tile * RADIX;
   for (int d = tid; d < RADIX; d += THREADS) {
     u32 run = 0;
 #pragma unroll
     for (int w = 0; w < WARPS; ++w) {
       const u32 c = whist[w * RADIX + d];
-      whist[w * RADIX + d] = (uint16_t)run;
+      whist[w * RADIX + d] = run;
       run += c;
     }
     sexcl[d] = run;
+    sbase[d] = run;
+    st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | run);
   }
   __syncthreads();
+  block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
 
-  // Publish this tile's counts (tile 0: already inclusive); keep them in sbase.
-  u32* st = a.status + (u64)tile * RADIX;
-  for (int d = tid; d < RADIX; d += THREADS) {
-    const u32 c = sexcl[d];
-    sbase[d] = c;
-    st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | c);
-  }
-  block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);
-
-  static_assert(TILE <= 8192 && RADIX <= 2048, "position/digit packing");
-#pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    const u32 d = rd[i] & 0xfffu;
-    // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
-    rd[i] = d < (u32)RADIX
-                ? 0x80000000u | (d << 13) | (sexcl[d] + (u32)whist[warp * RADIX + d] + (rd[i] >> 12))
-                : 0u;
-  }
-  __syncthreads();  // whist reads above are done before skeys (aliased) is written
-#pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    if (rd[i] & 0x80000000u) {
-      const u32 p = rd[i] & 0x1fffu;
-      skeys[p] = key[i];
-      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
-      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
-    }
-  }
-
-  // Resolve each digit's prefix over the earlier tiles and publish it.  The
-  // local sort above comes first: it gives earlier tiles time to publish, so
-  // the walk back rarely has to wait.
+  // Resolve each digit's prefix over the earlier tiles and publish it.
   constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
     const u32 c = sbase[d];
@@ -563,6 +565,43 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
     sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
   }
+
+  // Stable rank within the tile: lanes holding the same digit are ranked by
+  // lane, items are visited in row order and warps in row order (the
+  // per-warp counters start at the warp's exclusive prefix), so equal digits
+  // keep row order.  Peers are found with one ballot per digit bit; the
+  // lowest peer advances the warp's counter for the whole group.
+  static_assert(TILE <= 8192 && RADIX <= 2048, "position/digit packing");
+  const u32 lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 d = rd[i];
+    const bool valid = d < (u32)RADIX;
+    u32 peers = __ballot_sync(0xffffffffu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const u32 bit = (d >> b) & 1u;
+      const u32 bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
+    const int leader = 31 - __clz(peers);
+    u32 prior = 0;
+    if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
+    prior = __shfl_sync(0xffffffffu, prior, leader);
+    // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
+    rd[i] = valid ? 0x80000000u | (d << 13) | (sexcl[d] + prior + __popc(peers & lt)) : 0u;
+  }
+  __syncthreads();  // whist reads above are done before skeys (aliased) is written
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    if (rd[i] & 0x80000000u) {
+      const u32 p = rd[i] & 0x1fffu;
+      skeys[p] = key[i];
+      sidx[p] = (uint16_t)(warp * 32 * IPT + i * 32 + lane);
+      sdig[p] = (uint16_t)((rd[i] >> 13) & 0xfffu);
+    }
+  }
   cp_async_wait_all();
   __syncthreads();
   if (sflag[1]) return;
@@ -570,6 +609,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   K* kout = (K*)a.keys_out;
   const bool plain_out = !a.raw_out && !a.reverse && !(a.segmented && a.seg.key_shift_q);
   if (full && plain_out) {
+    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
     // full tile: IPT independent slots per thread, loads before stores
 #pragma unroll
     for (int i0 = 0; i0 < IPT; i0 += 8) {
@@ -584,8 +624,8 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
       }
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const u64 g = gg[i];
-        if (g < seg_row0 || g >= seg_row1) {
+        const u32 g = gg[i];  // rows < 2^30: 32-bit positions
+        if (g - row0 >= span) {
           atomicOr(a.err, DERR_BOUNDS);
           continue;
         }
@@ -783,6 +823,10 @@ __global__ void __launch_bounds__(256) k_minmax(PackDesc pd, u64 n, u64* out) {
       }
     }
   }
+  // warp, then block reduction: one pair of global atomics per block and
+  // column (every block hits the same two words, so they serialise in L2)
+  __shared__ u64 smn[kMaxCols][8], smx[kMaxCols][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int j = 0; j < kMaxCols; ++j) {
     if (j >= pd.ncols) break;
@@ -794,10 +838,21 @@ __global__ void __launch_bounds__(256) k_minmax(PackDesc pd, u64 n, u64* out) {
       a = a2 < a ? a2 : a;
       b = b2 > b ? b2 : b;
     }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMin(&out[2 * j], a);
-      atomicMax(&out[2 * j + 1], b);
+    if (lane == 0) {
+      smn[j][warp] = a;
+      smx[j][warp] = b;
     }
+  }
+  __syncthreads();
+  if (threadIdx.x < pd.ncols) {
+    const int j = threadIdx.x;
+    u64 a = smn[j][0], b = smx[j][0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      a = smn[j][w] < a ? smn[j][w] : a;
+      b = smx[j][w] > b ? smx[j][w] : b;
+    }
+    atomicMin(&out[2 * j], a);
+    atomicMax(&out[2 * j + 1], b);
   }
 }
 
