@@ -153,6 +153,28 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
 int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out,
                     void* const* keys_out, void* stream);
 
+/* A payload column gathered by jfx_join_expand_gather as the rows are
+ * written: out[i] = data[row] of the output row's left (side 0) or right
+ * (side 1) row, converted to out_dtype; a missing row (-1) gives NaN for a
+ * float output and -1 otherwise -- the gathers of ParallelSortMergeJoin.join
+ * (:1056-1073), which jfx_gather also implements. */
+typedef struct {
+  const void* data; /* device pointer, n rows of the side's table, original order */
+  int64_t n;
+  int32_t dtype;
+  int32_t side;     /* 0 = left table, 1 = right table */
+  void* out;        /* device pointer, num_out elements of out_dtype */
+  int32_t out_dtype;
+  int32_t reserved;
+} jfx_join_payload;
+
+/* jfx_join_expand plus up to 8 payload gathers in the same kernel (inner,
+ * left and right joins; outer joins use jfx_join_expand + jfx_gather).
+ * left_idx_out / right_idx_out may be null here. */
+int jfx_join_expand_gather(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out,
+                           void* const* keys_out, const jfx_join_payload* payloads, int npayloads,
+                           void* stream);
+
 /* Rows of one side (0 = left, 1 = right) that have no match, in ascending row
  * order, as join_multi_column appends them (:883-917).  *count receives the
  * number after one stream synchronisation; rows_out needs that capacity. */
@@ -225,11 +247,15 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
 int jfx_batch_status(void* workspace, size_t workspace_bytes, void* stream);
 
 /* Tuning of this thread's later calls (no counterpart in the reference): the
- * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width)).
- * jfx_set_tuning(NULL) restores the defaults.  The autotuner
- * (jaxframes_b200/autotune.py) picks values per key dtype, size and skew. */
+ * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width))
+ * and whether the passes after the first run in two phases (per-tile digit
+ * counts and a scan first, then the pass without a look-back; 1, the
+ * default) or as single look-back passes (0).  jfx_set_tuning(NULL) restores
+ * the defaults.  The autotuner (jaxframes_b200/autotune.py) picks values per
+ * key dtype, size and skew. */
 typedef struct {
   int32_t max_digit_bits;
+  int32_t two_phase;
 } jfx_tuning;
 int jfx_set_tuning(const jfx_tuning* t);
 int jfx_get_tuning(jfx_tuning* t);

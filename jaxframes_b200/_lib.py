@@ -61,7 +61,13 @@ class AggColumn(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("max_digit_bits", ctypes.c_int32)]
+    _fields_ = [("max_digit_bits", ctypes.c_int32), ("two_phase", ctypes.c_int32)]
+
+
+class JoinPayload(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("n", ctypes.c_int64), ("dtype", ctypes.c_int32),
+                ("side", ctypes.c_int32), ("out", ctypes.c_void_p), ("out_dtype", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class JoinPlan(ctypes.Structure):
@@ -87,6 +93,8 @@ SIGNATURES = {
     "jfx_join_prepare": (_INT, [ctypes.POINTER(Column), _I64, ctypes.POINTER(Column), _I64, _INT, _INT,
                                 ctypes.POINTER(JoinPlan), ctypes.POINTER(_I64), _P, _SIZE, _P]),
     "jfx_join_expand": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, ctypes.POINTER(_P), _P]),
+    "jfx_join_expand_gather": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, ctypes.POINTER(_P),
+                                      ctypes.POINTER(JoinPayload), _INT, _P]),
     "jfx_join_unmatched": (_INT, [ctypes.POINTER(JoinPlan), _INT, _P, _I64, ctypes.POINTER(_I64), _P]),
     "jfx_coalesce": (_INT, [_P, _P, _I64, _P, _P, _I64, _I64, ctypes.c_int32, _P, _P]),
     "jfx_gather": (_INT, [_P, ctypes.c_int32, _I64, _P, _I64, _P, ctypes.c_int32, _P]),

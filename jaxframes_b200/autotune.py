@@ -140,12 +140,13 @@ class Autotuner:
 
 
 @contextlib.contextmanager
-def tuning(max_digit_bits: int | None = None):
+def tuning(max_digit_bits: int | None = None, two_phase: bool | None = None):
     """Applies a tuning to this thread's libjfx calls for the block."""
     L = _lib.load_library()
     old = _lib.Tuning()
     _lib.check(L.jfx_get_tuning(ctypes.byref(old)))
-    new = _lib.Tuning(old.max_digit_bits if max_digit_bits is None else int(max_digit_bits))
+    new = _lib.Tuning(old.max_digit_bits if max_digit_bits is None else int(max_digit_bits),
+                      old.two_phase if two_phase is None else int(bool(two_phase)))
     _lib.check(L.jfx_set_tuning(ctypes.byref(new)))
     try:
         yield

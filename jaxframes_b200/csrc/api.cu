@@ -119,6 +119,7 @@ struct JoinPlan {
   int key64;
   int ncols;
   int reverse_counted;  // counts with the sides swapped exist (lo2/cnt2)
+  int unique;           // inner join, every A row matches exactly once: output i = sorted A row i
   u64 nl, nr, m;
   u64 unmatched[2];     // rows without a match: [0] left, [1] right
   void* skL;
@@ -145,7 +146,7 @@ constexpr u64 kJoinMagic = 0x6a66786a6f696e32ull;
 struct JoinBuffers {
   void *skL, *skR;
   u32 *pL, *pR, *lo, *cnt, *lo2, *cnt2, *flag, *foff, *fpart, *ftotal;
-  u64 *off, *partial, *total, *win;
+  u64 *off, *partial, *total, *win, *stats;
 };
 static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
   take_common(ar, c);
@@ -167,11 +168,14 @@ static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, Joi
   j.fpart = ar.take<u32>(scan_partials_count(nmax));
   j.ftotal = ar.take<u32>(4);
   j.win = ar.take<u64>(2 * ((nmax + kJoinTile - 1) / kJoinTile + 1));
+  j.stats = ar.take<u64>(2 * kJoinStatSlots);
 }
 
 template <typename K>
+// stats (optional): kJoinStatSlots (sum, max) pairs of the counts; zeroed here.
 static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* lo, u32* cnt, const PackDesc& pd,
-                             u64* win, cudaStream_t s) {
+                             u64* win, cudaStream_t s, unsigned long long* stats = nullptr) {
+  if (stats) JFX_CUDA(cudaMemsetAsync(stats, 0, 2 * kJoinStatSlots * sizeof(unsigned long long), s));
   if (!na) return JFX_OK;
   if (!nb) {
     JFX_CUDA(cudaMemsetAsync(cnt, 0, na * sizeof(u32), s));
@@ -179,8 +183,8 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
     return JFX_OK;
   }
   const unsigned blocks = (unsigned)((na + kJoinTile - 1) / kJoinTile);
-  k_join_windows<K><<<(blocks + 255) / 256, 256, 0, s>>>((const K*)A, na, (const K*)B, nb, blocks, win), note_launch();
-  k_join_count<K><<<blocks, kJoinThreads, 0, s>>>((const K*)A, na, (const K*)B, nb, win, lo, cnt, pd), note_launch();
+  k_join_windows<K><<<(blocks + 7) / 8, 256, 0, s>>>((const K*)A, na, (const K*)B, nb, blocks, win), note_launch();
+  k_join_count<K><<<blocks, kJoinThreads, 0, s>>>((const K*)A, na, (const K*)B, nb, win, lo, cnt, pd, stats), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }
@@ -368,13 +372,16 @@ int jfx_set_tuning(const jfx_tuning* t) {
   }
   if (t->max_digit_bits < 8 || t->max_digit_bits > 11)
     return fail(JFX_ERR_ARG, "max_digit_bits must be in [8, 11], got %d", t->max_digit_bits);
+  if (t->two_phase != 0 && t->two_phase != 1) return fail(JFX_ERR_ARG, "two_phase must be 0 or 1, got %d", t->two_phase);
   g_tuning.max_digit_bits = t->max_digit_bits;
+  g_tuning.two_phase = t->two_phase;
   return JFX_OK;
 }
 
 int jfx_get_tuning(jfx_tuning* t) {
   if (!t) return fail(JFX_ERR_ARG, "null pointer");
   t->max_digit_bits = g_tuning.max_digit_bits;
+  t->two_phase = g_tuning.two_phase;
   return JFX_OK;
 }
 
@@ -846,22 +853,30 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   const u64 na = swap ? nr : nl, nb = swap ? nl : nr;
   const void* A = swap ? j.skR : j.skL;
   const void* B = swap ? j.skL : j.skR;
-  if (key64) JFX_TRY(launch_join_count<u64>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s));
-  else JFX_TRY(launch_join_count<u32>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s));
+  unsigned long long* stats = (unsigned long long*)j.stats;
+  if (key64) JFX_TRY(launch_join_count<u64>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s, stats));
+  else JFX_TRY(launch_join_count<u32>(A, na, B, nb, j.lo, j.cnt, pl, j.win, s, stats));
   const bool rev = how == JFX_JOIN_OUTER;
   if (rev) {
     if (key64) JFX_TRY(launch_join_count<u64>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, j.win, s));
     else JFX_TRY(launch_join_count<u32>(j.skR, nr, j.skL, nl, j.lo2, j.cnt2, pl, j.win, s));
   }
-  host[1] = 0;
-  if (na && nb) {
-    JFX_TRY(device_exclusive_scan<u64>(j.cnt, na, j.off, j.total, j.partial, s));
-    JFX_CUDA(cudaMemcpyAsync(host + 1, j.total, sizeof(u64), cudaMemcpyDeviceToHost, s));
-  }
+  // one synchronisation: error word, sum of the counts (= inner pairs) and
+  // the largest count
+  JFX_CUDA(cudaMemcpyAsync(host + 8, stats, 2 * kJoinStatSlots * sizeof(u64), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaStreamSynchronize(s));
   JFX_TRY(check_err_word((u32)host[0]));
+  host[1] = host[2] = 0;
+  for (int k = 0; k < kJoinStatSlots; ++k) {
+    host[1] += host[8 + 2 * k];
+    host[2] = std::max(host[2], host[8 + 2 * k + 1]);
+  }
   const u64 inner = (na && nb) ? host[1] : 0;
+  // many-to-one inner join with every row matched: no offsets are needed
+  const bool unique = how == JFX_JOIN_INNER && na && nb && host[2] <= 1 && inner == na;
+  if ((how == JFX_JOIN_INNER || how == JFX_JOIN_OUTER) && !unique && na && nb)
+    JFX_TRY(device_exclusive_scan<u64>(j.cnt, na, j.off, j.total, j.partial, s));
   u64 m = how == JFX_JOIN_INNER || how == JFX_JOIN_OUTER ? inner : na;
   if (m > (u64)0x7fffffffull) return fail(JFX_ERR_CAPACITY, "join produces %llu rows; at most 2^31-1 are supported", m);
   JoinPlan* jp = (JoinPlan*)plan_out;
@@ -871,6 +886,7 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   jp->key64 = key64;
   jp->ncols = ncols;
   jp->reverse_counted = rev;
+  jp->unique = unique;
   jp->nl = (u64)nl;
   jp->nr = (u64)nr;
   jp->m = m;
@@ -897,14 +913,11 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   return JFX_OK;
 }
 
-int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out, void* const* keys_out,
-                    void* stream) {
-  if (!plan) return fail(JFX_ERR_ARG, "null plan");
-  const JoinPlan* jp = (const JoinPlan*)plan;
-  if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
-  if (jp->m == 0) return JFX_OK;
-  if (!left_idx_out || !right_idx_out) return fail(JFX_ERR_ARG, "null index output");
-  cudaStream_t s = as_stream(stream);
+}  // extern "C"
+
+// Shared body of jfx_join_expand and jfx_join_expand_gather.
+static int join_expand(const JoinPlan* jp, int32_t* left_idx_out, int32_t* right_idx_out, void* const* keys_out,
+                       const JoinPayloads& pay, cudaStream_t s) {
   const bool swap = jp->how == JFX_JOIN_RIGHT;
   JoinKeyOut ko;
   memset(&ko, 0, sizeof ko);
@@ -919,26 +932,77 @@ int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* r
   const u32* pB = swap ? jp->pL : jp->pR;
   int32_t* a_out = swap ? right_idx_out : left_idx_out;
   int32_t* b_out = swap ? left_idx_out : right_idx_out;
-  if (jp->how == JFX_JOIN_INNER || jp->how == JFX_JOIN_OUTER) {
+  if (jp->unique) {
+    const int g = grid_for(na, 256);
+    if (jp->key64)
+      k_join_expand_unique<u64><<<g, 256, 0, s>>>(na, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko, pay), note_launch();
+    else
+      k_join_expand_unique<u32><<<g, 256, 0, s>>>(na, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko, pay), note_launch();
+  } else if (jp->how == JFX_JOIN_INNER || jp->how == JFX_JOIN_OUTER) {
     // output tiles in chunks of the window buffer's capacity
     const u64 tiles = (jp->m + kJoinTile - 1) / kJoinTile;
     for (u64 t0 = 0; t0 < tiles; t0 += jp->win_cap) {
       const unsigned blocks = (unsigned)std::min<u64>(jp->win_cap, tiles - t0);
-      k_expand_windows<<<(blocks + 255) / 256, 256, 0, s>>>(jp->off, na, jp->m, t0, blocks, jp->win), note_launch();
+      k_expand_windows<<<(blocks + 7) / 8, 256, 0, s>>>(jp->off, na, jp->m, t0, blocks, jp->win), note_launch();
       if (jp->key64)
-        k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko, t0), note_launch();
+        k_join_expand_inner<u64><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko, pay, t0), note_launch();
       else
-        k_join_expand_inner<u32><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko, t0), note_launch();
+        k_join_expand_inner<u32><<<blocks, kJoinThreads, 0, s>>>(jp->off, na, jp->m, jp->win, jp->lo, pA, pB, (const u32*)skA, a_out, b_out, ko, pay, t0), note_launch();
     }
   } else {
     const int g = grid_for(na, 256);
     if (jp->key64)
-      k_join_expand_first<u64><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u64*)skA, a_out, b_out, ko), note_launch();
+      k_join_expand_first<u64><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u64*)skA, a_out, b_out, ko, pay), note_launch();
     else
-      k_join_expand_first<u32><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u32*)skA, a_out, b_out, ko), note_launch();
+      k_join_expand_first<u32><<<g, 256, 0, s>>>(na, jp->lo, jp->cnt, pA, pB, (const u32*)skA, a_out, b_out, ko, pay), note_launch();
   }
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
+}
+
+extern "C" {
+
+int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out, void* const* keys_out,
+                    void* stream) {
+  if (!plan) return fail(JFX_ERR_ARG, "null plan");
+  const JoinPlan* jp = (const JoinPlan*)plan;
+  if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
+  if (jp->m == 0) return JFX_OK;
+  if (!left_idx_out || !right_idx_out) return fail(JFX_ERR_ARG, "null index output");
+  JoinPayloads pay;
+  memset(&pay, 0, sizeof pay);
+  return join_expand(jp, left_idx_out, right_idx_out, keys_out, pay, as_stream(stream));
+}
+
+int jfx_join_expand_gather(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* right_idx_out,
+                           void* const* keys_out, const jfx_join_payload* payloads, int npayloads, void* stream) {
+  if (!plan) return fail(JFX_ERR_ARG, "null plan");
+  const JoinPlan* jp = (const JoinPlan*)plan;
+  if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
+  if (npayloads < 0 || npayloads > kMaxJoinPayloads)
+    return fail(JFX_ERR_ARG, "0..%d payload columns per call, got %d", kMaxJoinPayloads, npayloads);
+  if (npayloads && !payloads) return fail(JFX_ERR_ARG, "null payload array");
+  if (jp->how == JFX_JOIN_OUTER) return fail(JFX_ERR_ARG, "outer joins gather their payloads with jfx_gather");
+  JoinPayloads pay;
+  memset(&pay, 0, sizeof pay);
+  pay.n = npayloads;
+  pay.swap = jp->how == JFX_JOIN_RIGHT;
+  for (int k = 0; k < npayloads; ++k) {
+    const jfx_join_payload& q = payloads[k];
+    if (q.side != 0 && q.side != 1) return fail(JFX_ERR_ARG, "payload %d: side must be 0 (left) or 1 (right)", k);
+    if (dtype_size(q.dtype) == 0 || dtype_size(q.out_dtype) == 0) return fail(JFX_ERR_DTYPE, "payload %d: unsupported dtype", k);
+    const u64 rows = q.side ? jp->nr : jp->nl;
+    if (q.n != (int64_t)rows) return fail(JFX_ERR_ARG, "payload %d has %lld rows, its table %llu", k, (long long)q.n, rows);
+    if ((!q.data && rows) || (!q.out && jp->m)) return fail(JFX_ERR_ARG, "payload %d: null pointer", k);
+    pay.src[k] = q.data;
+    pay.out[k] = q.out;
+    pay.n_src[k] = rows;
+    pay.sdt[k] = q.dtype;
+    pay.odt[k] = q.out_dtype;
+    pay.side[k] = q.side;
+  }
+  if (jp->m == 0) return JFX_OK;
+  return join_expand(jp, left_idx_out, right_idx_out, keys_out, pay, as_stream(stream));
 }
 
 int jfx_join_unmatched(const jfx_join_plan* plan, int side, int32_t* rows_out, int64_t capacity, int64_t* count,

@@ -152,6 +152,11 @@ struct PassArgs {
   int segmented;
   SegTables seg;
   PackDesc pack;
+  // two-phase pass: [RADIX][tiles] global position of each tile's first key
+  // of each digit, computed beforehand (k_tile_count + k_tile_scan); the
+  // pass then needs no look-back and takes tile ids from blockIdx
+  const u32* tile_base;
+  u64 ntiles;
 };
 
 __device__ __forceinline__ u32 fmix32(u32 h) {
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
-    sflag[0] = atomicAdd(a.tile_counter, 1u);
+    sflag[0] = a.tile_base ? blockIdx.x : atomicAdd(a.tile_counter, 1u);
     sflag[1] = 0;
   }
   for (int i = tid; i < WARPS * RADIX; i += THREADS) whist[i] = 0u;
@@ -546,7 +551,7 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
     }
     sexcl[d] = run;
     sbase[d] = run;
-    st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | run);
+    if (!a.tile_base) st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | run);
   }
   __syncthreads();
   block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
@@ -554,6 +559,10 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   // Resolve each digit's prefix over the earlier tiles and publish it.
   constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
+    if (a.tile_base) {  // two-phase pass: the tile's digit bases are known
+      sbase[d] = (u32)seg_row0 + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
+      continue;
+    }
     const u32 c = sbase[d];
     u32 excl = 0;
     bool bad = false;
@@ -767,6 +776,53 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
     if (sh[i]) atomicAdd(&a.hist[i], sh[i]);
 }
 
+// k_hist for the common key: one plain 32/64-bit integer column, digits of
+// its packed value.  T is the column's storage type.  The dtype dispatch and
+// the transform are fixed per launch, so the loop body is a load, a sign flip,
+// a subtraction and one shared-memory atomic per pass.
+struct HistIntArgs {
+  const void* col;
+  u32* hist;  // [npass][RADIX], zeroed
+  u64 n;
+  u64 flip, tmin;
+  int kshift, npass;
+  int shift[8];
+  u32 mask[8];
+};
+
+template <typename K, typename T, int RB>
+__global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
+  constexpr int RADIX = 1 << RB;
+  extern __shared__ u32 sh[];
+  const int total = a.npass * RADIX;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) sh[i] = 0u;
+  __syncthreads();
+  const T* col = (const T*)a.col;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  constexpr int U = 8;  // rows per thread per step, loads issued together
+  for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < a.n; r0 += stride * U) {
+    T raw[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const u64 r = r0 + (u64)u * stride;
+      raw[u] = r < a.n ? __ldg(col + r) : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (r0 + (u64)u * stride >= a.n) break;
+      const K k = (K)((((u64)raw[u] ^ a.flip) - a.tmin) << a.kshift);
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        if (p >= a.npass) break;
+        atomicAdd(&sh[p * RADIX + ((u32)(k >> a.shift[p]) & a.mask[p])], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < total; i += blockDim.x)
+    if (sh[i]) atomicAdd(&a.hist[i], sh[i]);
+}
+
 // Exclusive scan of each pass's histogram (one CTA per pass).
 template <int RB>
 __global__ void __launch_bounds__(1024) k_hist_scan(const u32* hist, u32* base) {
@@ -778,6 +834,91 @@ __global__ void __launch_bounds__(1024) k_hist_scan(const u32* hist, u32* base) 
   __syncthreads();
   block_exclusive_scan<1024, RADIX>(data, scratch);
   for (int i = threadIdx.x; i < RADIX; i += 1024) base[(u64)blockIdx.x * RADIX + i] = data[i];
+}
+
+// ------------------------------------------------------ two-phase passes ---
+// A later pass can do without the decoupled look-back: k_tile_count counts
+// each tile's digits, k_tile_scan turns the counts into every tile's global
+// base per digit (column-wise exclusive scan plus the digit's global offset),
+// and the pass reads its bases instead of waiting on earlier tiles.  That
+// costs one more read of the keys, but no tile ever waits on another.
+
+// counts[d][tile] (digit-major, so the scan reads rows) of digit
+// (key >> shift) & mask; one CTA per tile.
+template <typename K, int RB>
+__global__ void __launch_bounds__(256) k_tile_count(const K* keys, u64 n, int shift, u32 mask, u32* counts,
+                                                    u64 tiles) {
+  constexpr int RADIX = 1 << RB, TILE = PassLayout<K, RB>::TILE, IPT = TILE / 256;
+  constexpr int NH = RB <= 9 ? 8 : RB == 10 ? 4 : 2;  // histogram copies (fewer same-address atomics)
+  __shared__ u32 h[NH][RADIX];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < NH * RADIX; i += 256) (&h[0][0])[i] = 0u;
+  const u64 base = (u64)blockIdx.x * TILE;
+  const u32 tile_n = (u32)min((u64)TILE, n - base);
+  const K* src = keys + base + warp * 32 * IPT + lane;
+  K k[IPT];
+  if (tile_n == (u32)TILE) {
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) k[i] = src[i * 32];
+  } else {
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) k[i] = (warp * 32 * IPT + i * 32 + lane) < tile_n ? src[i * 32] : (K)0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < IPT; ++i)
+    if ((warp * 32 * IPT + i * 32 + lane) < tile_n) atomicAdd(&h[warp % NH][(u32)(k[i] >> shift) & mask], 1u);
+  __syncthreads();
+  for (int d = tid; d < RADIX; d += 256) {
+    u32 c = 0;
+#pragma unroll
+    for (int w = 0; w < NH; ++w) c += h[w][d];
+    counts[(u64)d * tiles + blockIdx.x] = c;
+  }
+}
+
+// base[d][t] = bin_base[d] + sum over t' < t of counts[d][t'] (mod 2^32:
+// rows < 2^30).  One CTA per digit row, 4096 tiles per round.
+template <int RB>
+__global__ void __launch_bounds__(256) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base) {
+  constexpr int PER = 16;
+  __shared__ u32 wsum[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32* row = counts + (u64)blockIdx.x * tiles;
+  u32* out = base + (u64)blockIdx.x * tiles;
+  u32 carry = bin_base[blockIdx.x];
+  for (u64 c0 = 0; c0 < tiles; c0 += 256 * PER) {
+    const u64 t0 = c0 + (u64)tid * PER;
+    u32 v[PER];
+    u32 sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      v[k] = t0 + k < tiles ? row[t0 + k] : 0u;
+      sum += v[k];
+    }
+    u32 x = sum;  // inclusive scan of the thread sums: warp, then block
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    u32 wpre = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      wpre += w < warp ? wsum[w] : 0u;
+      total += wsum[w];
+    }
+    u32 run = carry + wpre + x - sum;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      if (t0 + k < tiles) out[t0 + k] = run;
+      run += v[k];
+    }
+    carry += total;
+    __syncthreads();  // wsum is rewritten next round
+  }
 }
 
 // ---------------------------------------------------------------- min/max ---
@@ -856,6 +997,52 @@ __global__ void __launch_bounds__(256) k_minmax(PackDesc pd, u64 n, u64* out) {
   }
 }
 
+// Min/max of one plain 32/64-bit integer column's transformed value (the
+// sign flip is the whole transform), T its storage type.
+template <typename T>
+__global__ void __launch_bounds__(256) k_minmax_int(const T* col, u64 n, u64 flip, u64* out) {
+  u64 mn = ~0ull, mx = 0ull;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  constexpr int U = 8;
+  for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += stride * U) {
+    T raw[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const u64 r = r0 + (u64)u * stride;
+      raw[u] = r < n ? __ldg(col + r) : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (r0 + (u64)u * stride >= n) break;
+      const u64 t = (u64)raw[u] ^ flip;
+      mn = t < mn ? t : mn;
+      mx = t > mx ? t : mx;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const u64 a2 = __shfl_xor_sync(0xffffffffu, mn, o);
+    const u64 b2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mn = a2 < mn ? a2 : mn;
+    mx = b2 > mx ? b2 : mx;
+  }
+  __shared__ u64 smn[8], smx[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smn[warp] = mn;
+    smx[warp] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      mn = smn[w] < mn ? smn[w] : mn;
+      mx = smx[w] > mx ? smx[w] : mx;
+    }
+    atomicMin(&out[0], mn);
+    atomicMax(&out[1], mx);
+  }
+}
+
 __global__ void k_init_minmax(u64* out, int ncols) {
   int j = threadIdx.x;
   if (j < ncols) {
@@ -879,6 +1066,7 @@ __global__ void k_fill_keys(K* out, u64 n) {
 // Thread-local tuning (jfx_set_tuning): widest radix digit of a pass.
 struct Tuning {
   int max_digit_bits = 8;
+  int two_phase = 1;  // later radix passes: counts + scan, no look-back
 };
 extern thread_local Tuning g_tuning;
 
@@ -924,7 +1112,16 @@ inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s
   k_init_minmax<<<1, 32, 0, s>>>(dev_out, pd.ncols), note_launch();
   if (n) {
     int grid = (int)std::min<u64>((n + 255) / 256, (u64)device_sm_count() * 8);
-    k_minmax<<<grid, 256, 0, s>>>(pd, n, dev_out), note_launch();
+    const int d0 = pd.c[0].dtype;
+    const bool int_key = pd.ncols == 1 && !(pd.c[0].flags & CF_DESC) &&
+                         (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
+    const u64 flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
+    if (int_key && (d0 == JFX_I64 || d0 == JFX_U64))
+      k_minmax_int<u64><<<grid, 256, 0, s>>>((const u64*)pd.c[0].ptr, n, flip, dev_out), note_launch();
+    else if (int_key)
+      k_minmax_int<u32><<<grid, 256, 0, s>>>((const u32*)pd.c[0].ptr, n, flip, dev_out), note_launch();
+    else
+      k_minmax<<<grid, 256, 0, s>>>(pd, n, dev_out), note_launch();
   }
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
@@ -1112,14 +1309,42 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     static bool attr = false;
     if (!attr) {
       JFX_CUDA(cudaFuncSetAttribute(k_hist<K, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
+      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u64, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
+      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u32, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
       attr = true;
     }
-    k_hist<K, RB><<<std::max(grid, 1), 256, smem, s>>>(h), note_launch();
+    const int d0 = rq.pack.c[0].dtype;
+    const bool int_key = rq.pack.ncols == 1 && rq.key_mode == KEY_PACK && rq.digit_mode == DIG_BITS &&
+                         !rq.targets && !(rq.pack.c[0].flags & CF_DESC) &&
+                         (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
+    if (int_key) {
+      HistIntArgs hi;
+      memset(&hi, 0, sizeof hi);
+      hi.col = rq.pack.c[0].ptr;
+      hi.hist = b.hist;
+      hi.n = n;
+      hi.flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
+      hi.tmin = rq.pack.c[0].tmin;
+      hi.kshift = rq.pack.c[0].shift;
+      hi.npass = npass;
+      for (int p = 0; p < 8; ++p) {
+        hi.shift[p] = shift[p];
+        hi.mask[p] = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
+      }
+      if (d0 == JFX_I64 || d0 == JFX_U64)
+        k_hist_int<K, u64, RB><<<std::max(grid, 1), 256, smem, s>>>(hi), note_launch();
+      else
+        k_hist_int<K, u32, RB><<<std::max(grid, 1), 256, smem, s>>>(hi), note_launch();
+    } else {
+      k_hist<K, RB><<<std::max(grid, 1), 256, smem, s>>>(h), note_launch();
+    }
     JFX_CUDA(cudaGetLastError());
   }
   k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
   JFX_CUDA(cudaGetLastError());
 
+  // later passes of a plain digit sort run in two phases (no look-back)
+  const bool two_phase = rq.digit_mode == DIG_BITS && g_tuning.two_phase && tiles >= 2;
   u32* out_vals[kMaxWords];
   for (int w = 0; w < kMaxWords; ++w) out_vals[w] = rq.vout_final[w];
   if (!out_vals[0]) out_vals[0] = rq.perm_out;
@@ -1157,6 +1382,20 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       a.raw_tmin = rq.raw_tmin;
     }
     a.pack = rq.pack;
+    if (two_phase && p > 0) {
+      // status[1] holds this pass's tile counts, status[0] its tile bases
+      // (pass 0, the only look-back pass, is done with both by now)
+      const u32 mask_p = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
+      k_tile_count<K, RB><<<(unsigned)tiles, 256, 0, s>>>((const K*)a.keys_in, n, shift[p], mask_p, b.status[1],
+                                                           tiles), note_launch();
+      k_tile_scan<RB><<<RADIX, 256, 0, s>>>(b.status[1], tiles, a.bin_base, b.status[0]), note_launch();
+      JFX_CUDA(cudaGetLastError());
+      a.tile_base = b.status[0];
+      a.ntiles = tiles;
+      a.status = nullptr;
+      a.status_next = nullptr;
+    }
+    if (two_phase && p == 0) a.status_next = nullptr;
     if (p == 0) {
       JFX_TRY((launch_pass<K, RB, true, NW>(a, n, s)));
     } else {

@@ -399,6 +399,34 @@ def _join_expand(plan, m, like, key_cols=None):
     return li, ri, outs
 
 
+def _join_expand_gather(plan, m, like, key_col, payloads):
+    """Merged keys plus the payload columns of ``join`` in one expand kernel
+    per 8 payloads.  payloads: [(name, tensor, side 0/1, out dtype)]."""
+    L = _lib.lib()
+    mk = _empty(m, key_col.dtype, like)
+    outs = {name: _empty(m, odt, like) for name, _, _, odt in payloads}
+    if m:
+        chunks = [payloads[i:i + 8] for i in range(0, len(payloads), 8)] or [[]]
+        for ci, chunk in enumerate(chunks):
+            arr = (_lib.JoinPayload * max(len(chunk), 1))()
+            for k, (name, t, side, odt) in enumerate(chunk):
+                arr[k] = _lib.JoinPayload(t.data_ptr() if t.numel() else None, t.numel(), _lib.jfx_dtype(t), side,
+                                          outs[name].data_ptr(), _lib.TORCH_TO_JFX[odt], 0)
+            keys = (ctypes.c_void_p * 1)(mk.data_ptr()) if ci == 0 else None
+            check(L.jfx_join_expand_gather(ctypes.byref(plan), None, None, keys, arr, len(chunk), _stream()))
+    return mk, outs
+
+
+_SIDE_STREAMS = {}
+
+
+def _side_stream(dev):
+    s = _SIDE_STREAMS.get(dev)
+    if s is None:
+        s = _SIDE_STREAMS[dev] = torch.cuda.Stream(device=dev)
+    return s
+
+
 def _join_unmatched(plan, side: int, n: int, like):
     L = _lib.lib()
     out = _empty(max(n, 1), torch.int32, like)
@@ -476,14 +504,41 @@ class ParallelSortMergeJoin:
         """Line 938-1075: ``(merged_keys, {left_<col>, right_<col>})``; payloads
         go through ``where(idx >= 0, col[idx], nan)``, so integer payloads
         become the default float even for an inner join."""
-        mk, li, ri = self.join_indices(left_keys, right_keys, how)
-        out = {}
-        for c, a in left_values.items():
-            t = as_device(a)
-            out[f"left_{c}"] = _gather(t, li, t.dtype if _is_float(t) else config.default_float())
-        for c, a in right_values.items():
-            t = as_device(a)
-            out[f"right_{c}"] = _gather(t, ri, t.dtype if _is_float(t) else config.default_float())
+        if how not in _lib.JOIN_KINDS:
+            raise ValueError(f"Unsupported join type: {how}")
+        if how == "outer":
+            mk, li, ri = self.join_indices(left_keys, right_keys, how)
+            out = {}
+            for c, a in left_values.items():
+                t = as_device(a)
+                out[f"left_{c}"] = _gather(t, li, t.dtype if _is_float(t) else config.default_float())
+            for c, a in right_values.items():
+                t = as_device(a)
+                out[f"right_{c}"] = _gather(t, ri, t.dtype if _is_float(t) else config.default_float())
+            return mk, out
+        # keys first; host payload columns are copied on a side stream while
+        # the keys are sorted, and gathered inside the expand kernel
+        lk, rk = as_device(left_keys), as_device(right_keys)
+        cur = torch.cuda.current_stream(lk.device)
+        side = _side_stream(lk.device)
+        side.wait_stream(cur)
+        with torch.cuda.stream(side):
+            lv = {c: as_device(a, lk.device) for c, a in left_values.items()}
+            rv = {c: as_device(a, lk.device) for c, a in right_values.items()}
+        ready = torch.cuda.Event()
+        ready.record(side)
+        (lk,), (rk,) = _same_dtypes([lk], [rk])
+        plan, m, ws = _join_prepare([lk], [rk], how)
+        cur.wait_event(ready)
+        payloads = []
+        for c, t in lv.items():
+            t.record_stream(cur)
+            payloads.append((f"left_{c}", t, 0, t.dtype if _is_float(t) else config.default_float()))
+        for c, t in rv.items():
+            t.record_stream(cur)
+            payloads.append((f"right_{c}", t, 1, t.dtype if _is_float(t) else config.default_float()))
+        mk, out = _join_expand_gather(plan, m, lk, rk if how == "right" else lk, payloads)
+        del ws
         return mk, out
 
     def join_multi_indices(self, left_keys, right_keys, how: str = "inner"):

@@ -118,6 +118,33 @@ def test_radix_sort_matches_oracle(P, dt, kind):
             np.testing.assert_array_equal(_np(sk).view(np.uint8), ek.view(np.uint8), err_msg=f"n={n}")
 
 
+@pytest.mark.parametrize("two_phase", [0, 1])
+@pytest.mark.parametrize("dt", [np.int64, np.uint64, np.float32])
+def test_later_pass_modes_match_oracle(P, two_phase, dt):
+    """The passes after the first run either with a decoupled look-back or in
+    two phases (tile counts + scan, then the pass); both give the oracle's
+    order, including ragged last tiles, heavy digits and carried payloads."""
+    from jaxframes_b200.autotune import tuning
+    rng = np.random.default_rng(5 + two_phase)
+    with tuning(two_phase=bool(two_phase)):
+        for n in [4095, 4097, 8193, 250_001, 1_000_003]:
+            for kind in ("full", "heavy"):
+                k = _keys(rng, dt, n, kind)
+                sk, perm = P.ParallelRadixSort().sort(k, np.arange(n, dtype=np.int32), True)
+                ek, ep = O.radix_sort(k, np.arange(n), True)
+                np.testing.assert_array_equal(_np(perm), ep, err_msg=f"n={n} {kind}")
+                np.testing.assert_array_equal(_np(sk).view(np.uint8), ek.view(np.uint8), err_msg=f"n={n}")
+        n = 300_007
+        k1 = rng.integers(0, 50_000, n).astype(np.int32)
+        k2 = rng.integers(0, 64, n).astype(np.int32)
+        v = rng.integers(-1000, 1000, n).astype(np.int64)
+        uk, out = P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], {"v": v, "w": v}, {"v": "sum", "w": "min"})
+        ek, eout = O.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], {"v": v, "w": v}, {"v": "sum", "w": "min"})
+        np.testing.assert_array_equal(_np(uk["k1"]), ek["k1"])
+        np.testing.assert_array_equal(_np(out["v"]), eout["v"])
+        np.testing.assert_array_equal(_np(out["w"]), eout["w"])
+
+
 @pytest.mark.parametrize("ncols", [2, 3])
 def test_lexsort_matches_oracle(P, ncols):
     rng = np.random.default_rng(11 + ncols)
@@ -266,6 +293,29 @@ def test_join_c2_like_payloads(P):
         g = _np(out[c])
         assert g.dtype == eout[c].dtype
         np.testing.assert_array_equal(g, eout[c])
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "right"])
+def test_join_many_payloads_partial_matches(P, how):
+    """Unique right keys with half the left keys unmatched (the general expand,
+    not the every-row-matches one), ten payload columns of mixed dtypes (two
+    expand calls of at most 8 gathers)."""
+    rng = np.random.default_rng(11 + len(how))
+    nl, nr = 30_000, 12_000
+    lk = rng.integers(0, 2 * nr, nl).astype(np.int64)
+    rk = rng.permutation(nr).astype(np.int64)
+    dts = [np.float32, np.float64, np.int32, np.int64, np.uint8, np.int16, np.uint32, np.float32, np.int64, np.bool_]
+    mk_cols = lambda n: {f"c{i}": (rng.integers(0, 2, n).astype(dt) if dt == np.bool_ else
+                                   (rng.standard_normal(n) * 1000).astype(dt)) for i, dt in enumerate(dts)}
+    lv, rv = mk_cols(nl), mk_cols(nr)
+    mk, out = P.sort_merge_join(lk, lv, rk, rv, how)
+    emk, eout, _, _ = O.sort_merge_join(lk, lv, rk, rv, how)
+    np.testing.assert_array_equal(_np(mk), emk)
+    assert set(out) == set(eout)
+    for c in eout:
+        g = _np(out[c])
+        assert g.dtype == eout[c].dtype, c
+        np.testing.assert_array_equal(g, eout[c], err_msg=f"{how} {c}")
 
 
 @pytest.mark.parametrize("how", ["left", "right", "outer"])
