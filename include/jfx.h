@@ -168,6 +168,18 @@ typedef struct {
   int32_t reserved;
 } jfx_join_payload;
 
+/* jfx_join_prepare that also takes the payload columns jfx_join_expand_gather
+ * will write (their `out` is not used here).  A side whose payloads are all
+ * 4- or 8-byte and take at most 4 32-bit words in total carries them through
+ * its sort, so the expand reads them in sorted order instead of gathering
+ * them by row id (not for outer joins or float keys); that side keeps no row
+ * ids, so its index output must then be null.  No counterpart in the
+ * reference, where the gathers follow the join (:1056-1073). */
+int jfx_join_prepare_payloads(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys,
+                              int64_t nr, int ncols, int how, const jfx_join_payload* payloads,
+                              int npayloads, jfx_join_plan* plan, int64_t* num_out, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
 /* jfx_join_expand plus up to 8 payload gathers in the same kernel (inner,
  * left and right joins; outer joins use jfx_join_expand + jfx_gather).
  * left_idx_out / right_idx_out may be null here. */

@@ -93,6 +93,9 @@ SIGNATURES = {
     "jfx_join_prepare": (_INT, [ctypes.POINTER(Column), _I64, ctypes.POINTER(Column), _I64, _INT, _INT,
                                 ctypes.POINTER(JoinPlan), ctypes.POINTER(_I64), _P, _SIZE, _P]),
     "jfx_join_expand": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, ctypes.POINTER(_P), _P]),
+    "jfx_join_prepare_payloads": (_INT, [ctypes.POINTER(Column), _I64, ctypes.POINTER(Column), _I64, _INT, _INT,
+                                         ctypes.POINTER(JoinPayload), _INT, ctypes.POINTER(JoinPlan),
+                                         ctypes.POINTER(_I64), _P, _SIZE, _P]),
     "jfx_join_expand_gather": (_INT, [ctypes.POINTER(JoinPlan), _P, _P, ctypes.POINTER(_P),
                                       ctypes.POINTER(JoinPayload), _INT, _P]),
     "jfx_join_unmatched": (_INT, [ctypes.POINTER(JoinPlan), _INT, _P, _I64, ctypes.POINTER(_I64), _P]),

@@ -120,6 +120,10 @@ struct JoinPlan {
   int ncols;
   int reverse_counted;  // counts with the sides swapped exist (lo2/cnt2)
   int unique;           // inner join, every A row matches exactly once: output i = sorted A row i
+  int carried[2];       // words carried through the left / right sort (0: that side sorted row ids)
+  u32* cw[2][kMaxWords];
+  int npay;             // payload list given to prepare: side, dtype and first carried word
+  int pay_side[kMaxJoinPayloads], pay_dtype[kMaxJoinPayloads], pay_word[kMaxJoinPayloads];
   u64 nl, nr, m;
   u64 unmatched[2];     // rows without a match: [0] left, [1] right
   void* skL;
@@ -147,11 +151,12 @@ struct JoinBuffers {
   void *skL, *skR;
   u32 *pL, *pR, *lo, *cnt, *lo2, *cnt2, *flag, *foff, *fpart, *ftotal;
   u64 *off, *partial, *total, *win, *stats;
+  u32* cw[2][kMaxWords];  // carried payload words of each side, sorted order
 };
 static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
   take_common(ar, c);
   u64 nmax = std::max(nl, nr);
-  take_sort_buffers(ar, nmax, b);
+  take_sort_buffers(ar, nmax, b, kMaxWords);
   j.skL = ar.take<u64>(nl ? nl : 1);
   j.skR = ar.take<u64>(nr ? nr : 1);
   j.pL = ar.take<u32>(nl ? nl : 1);
@@ -169,6 +174,10 @@ static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, Joi
   j.ftotal = ar.take<u32>(4);
   j.win = ar.take<u64>(2 * ((nmax + kJoinTile - 1) / kJoinTile + 1));
   j.stats = ar.take<u64>(2 * kJoinStatSlots);
+  for (int w = 0; w < kMaxWords; ++w) {
+    j.cw[0][w] = ar.take<u32>(nl ? nl : 1);
+    j.cw[1][w] = ar.take<u32>(nr ? nr : 1);
+  }
 }
 
 template <typename K>
@@ -780,9 +789,12 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   return JFX_OK;
 }
 
-int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys, int64_t nr, int ncols,
-                     int how, jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
-                     void* stream) {
+}  // extern "C"
+
+// Shared body of jfx_join_prepare (no payloads) and jfx_join_prepare_payloads.
+static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys, int64_t nr,
+                        int ncols, int how, const jfx_join_payload* payloads, int npayloads, jfx_join_plan* plan_out,
+                        int64_t* num_out, void* workspace, size_t workspace_bytes, void* stream) {
   JFX_TRY(check_n(nl));
   JFX_TRY(check_n(nr));
   if (!left_keys || !right_keys || !plan_out || !num_out) return fail(JFX_ERR_ARG, "null argument");
@@ -829,23 +841,55 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   if (shift > 64) return fail(JFX_ERR_CAPACITY, "join keys need %d packed bits; at most 64 are supported", shift);
   const int total_bits = shift;
   const bool key64 = total_bits > 32;
-  if (nl) {
-    RadixRequest rq;
-    rq.pack = pl;
-    rq.total_bits = total_bits;
-    rq.key64 = key64;
-    rq.perm_out = j.pL;
-    rq.keys_out = j.skL;
-    JFX_TRY(radix_sort(rq, (u64)nl, b, c.err, s));
+  // Payload columns of a side ride through that side's sort as 32-bit words
+  // (4- and 8-byte dtypes, at most kMaxWords words) instead of being gathered
+  // by row id afterwards; then the side's row ids are not kept.  Not with a
+  // float key (its output is re-read by row id) nor for outer joins (their
+  // unmatched rows are found by row id).
+  int carried[2] = {0, 0};
+  int pay_word[kMaxJoinPayloads];
+  PayloadSrc psrc[2][kMaxWords];
+  memset(psrc, 0, sizeof psrc);
+  bool float_key = false;
+  for (int k = 0; k < ncols; ++k) float_key |= dtype_is_float(left_keys[k].dtype);
+  for (int side = 0; side < 2 && npayloads; ++side) {
+    int words = 0;
+    bool fits = how != JFX_JOIN_OUTER && !float_key;
+    for (int k = 0; k < npayloads; ++k) {
+      if (payloads[k].side != side) continue;
+      const int sz = dtype_size(payloads[k].dtype);
+      if (sz != 4 && sz != 8) fits = false;
+      words += sz / 4;
+    }
+    if (!fits || words == 0 || words > kMaxWords) continue;
+    int w = 0;
+    for (int k = 0; k < npayloads; ++k) {
+      if (payloads[k].side != side) continue;
+      const int sz = dtype_size(payloads[k].dtype);
+      pay_word[k] = w;
+      for (int h = 0; h < sz / 4; ++h) psrc[side][w++] = PayloadSrc{(const unsigned char*)payloads[k].data, (u32)sz, (u32)(4 * h)};
+    }
+    carried[side] = words;
   }
-  if (nr) {
+  for (int side = 0; side < 2; ++side) {
+    const u64 ns = side ? (u64)nr : (u64)nl;
+    if (!ns) continue;
     RadixRequest rq;
-    rq.pack = pr;
+    rq.pack = side ? pr : pl;
     rq.total_bits = total_bits;
     rq.key64 = key64;
-    rq.perm_out = j.pR;
-    rq.keys_out = j.skR;
-    JFX_TRY(radix_sort(rq, (u64)nr, b, c.err, s));
+    rq.keys_out = side ? j.skR : j.skL;
+    if (carried[side]) {
+      rq.total_bits = std::max(total_bits, 1);  // constant keys still run one pass to move the words
+      rq.nwords = carried[side];
+      for (int w = 0; w < carried[side]; ++w) {
+        rq.pfirst[w] = psrc[side][w];
+        rq.vout_final[w] = j.cw[side][w];
+      }
+    } else {
+      rq.perm_out = side ? j.pR : j.pL;
+    }
+    JFX_TRY(radix_sort(rq, ns, b, c.err, s));
   }
   // forward counts drive inner/left joins, swapped counts right joins; the
   // unmatched rows of a side need that side's counts
@@ -887,6 +931,16 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   jp->ncols = ncols;
   jp->reverse_counted = rev;
   jp->unique = unique;
+  jp->npay = npayloads;
+  for (int side = 0; side < 2; ++side) {
+    jp->carried[side] = carried[side];
+    for (int w = 0; w < kMaxWords; ++w) jp->cw[side][w] = carried[side] ? j.cw[side][w] : nullptr;
+  }
+  for (int k = 0; k < npayloads; ++k) {
+    jp->pay_side[k] = payloads[k].side;
+    jp->pay_dtype[k] = payloads[k].dtype;
+    jp->pay_word[k] = carried[payloads[k].side] ? pay_word[k] : -1;
+  }
   jp->nl = (u64)nl;
   jp->nr = (u64)nr;
   jp->m = m;
@@ -913,6 +967,34 @@ int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* 
   return JFX_OK;
 }
 
+extern "C" {
+
+int jfx_join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys, int64_t nr, int ncols,
+                     int how, jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
+                     void* stream) {
+  return join_prepare(left_keys, nl, right_keys, nr, ncols, how, nullptr, 0, plan_out, num_out, workspace,
+                      workspace_bytes, stream);
+}
+
+int jfx_join_prepare_payloads(const jfx_column* left_keys, int64_t nl, const jfx_column* right_keys, int64_t nr,
+                              int ncols, int how, const jfx_join_payload* payloads, int npayloads,
+                              jfx_join_plan* plan_out, int64_t* num_out, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+  if (npayloads < 0 || npayloads > kMaxJoinPayloads)
+    return fail(JFX_ERR_ARG, "0..%d payload columns per call, got %d", kMaxJoinPayloads, npayloads);
+  if (npayloads && !payloads) return fail(JFX_ERR_ARG, "null payload array");
+  for (int k = 0; k < npayloads; ++k) {
+    const jfx_join_payload& q = payloads[k];
+    if (q.side != 0 && q.side != 1) return fail(JFX_ERR_ARG, "payload %d: side must be 0 (left) or 1 (right)", k);
+    if (dtype_size(q.dtype) == 0) return fail(JFX_ERR_DTYPE, "payload %d: unsupported dtype", k);
+    if (q.n != (q.side ? nr : nl)) return fail(JFX_ERR_ARG, "payload %d has %lld rows, its table %lld", k,
+                                               (long long)q.n, (long long)(q.side ? nr : nl));
+    if (!q.data && q.n) return fail(JFX_ERR_ARG, "payload %d: null pointer", k);
+  }
+  return join_prepare(left_keys, nl, right_keys, nr, ncols, how, payloads, npayloads, plan_out, num_out, workspace,
+                      workspace_bytes, stream);
+}
+
 }  // extern "C"
 
 // Shared body of jfx_join_expand and jfx_join_expand_gather.
@@ -925,6 +1007,14 @@ static int join_expand(const JoinPlan* jp, int32_t* left_idx_out, int32_t* right
   for (int k = 0; k < jp->ncols; ++k) {
     ko.out[k] = keys_out ? keys_out[k] : nullptr;
     ko.c[k] = swap ? jp->rc[k] : jp->lc[k];
+    if (ko.out[k] && dtype_is_float(ko.c[k].dtype)) ko.float_key = 1;
+  }
+  {
+    const int dt = ko.c[0].dtype;
+    if (jp->ncols == 1 && ko.out[0] && (dt == JFX_I32 || dt == JFX_I64 || dt == JFX_U32 || dt == JFX_U64)) {
+      ko.fast_size = dtype_size(dt);
+      ko.fast_flip = dt == JFX_I64 ? 0x8000000000000000ull : dt == JFX_I32 ? 0x80000000ull : 0ull;
+    }
   }
   const u64 na = swap ? jp->nr : jp->nl;
   const void* skA = swap ? jp->skR : jp->skL;
@@ -969,6 +1059,8 @@ int jfx_join_expand(const jfx_join_plan* plan, int32_t* left_idx_out, int32_t* r
   if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
   if (jp->m == 0) return JFX_OK;
   if (!left_idx_out || !right_idx_out) return fail(JFX_ERR_ARG, "null index output");
+  if (jp->carried[0] || jp->carried[1])
+    return fail(JFX_ERR_ARG, "this plan carried payloads through the sorts and kept no row ids: use jfx_join_expand_gather");
   JoinPayloads pay;
   memset(&pay, 0, sizeof pay);
   return join_expand(jp, left_idx_out, right_idx_out, keys_out, pay, as_stream(stream));
@@ -1000,7 +1092,22 @@ int jfx_join_expand_gather(const jfx_join_plan* plan, int32_t* left_idx_out, int
     pay.sdt[k] = q.dtype;
     pay.odt[k] = q.out_dtype;
     pay.side[k] = q.side;
+    pay.kind[k] = payload_kind(q.dtype, q.out_dtype);
+    if (jp->carried[q.side]) {
+      // the side's payloads were carried: this list must be the one given to prepare
+      if (npayloads != jp->npay || jp->pay_side[k] != q.side || jp->pay_dtype[k] != q.dtype || jp->pay_word[k] < 0)
+        return fail(JFX_ERR_ARG, "payload %d does not match the list given to jfx_join_prepare_payloads", k);
+      pay.cw0[k] = jp->cw[q.side][jp->pay_word[k]];
+      pay.cw1[k] = dtype_size(q.dtype) == 8 ? jp->cw[q.side][jp->pay_word[k] + 1] : nullptr;
+    } else {
+      pay.gathered = 1;
+    }
   }
+  bool need_rows[2] = {left_idx_out != nullptr, right_idx_out != nullptr};
+  for (int k = 0; k < npayloads; ++k)
+    if (!pay.cw0[k]) need_rows[payloads[k].side] = true;
+  if ((need_rows[0] && jp->carried[0]) || (need_rows[1] && jp->carried[1]))
+    return fail(JFX_ERR_ARG, "row ids were not kept for a side whose payloads were carried; pass null index outputs");
   if (jp->m == 0) return JFX_OK;
   return join_expand(jp, left_idx_out, right_idx_out, keys_out, pay, as_stream(stream));
 }
@@ -1011,6 +1118,7 @@ int jfx_join_unmatched(const jfx_join_plan* plan, int side, int32_t* rows_out, i
   const JoinPlan* jp = (const JoinPlan*)plan;
   if (jp->magic != kJoinMagic) return fail(JFX_ERR_ARG, "plan was not filled by jfx_join_prepare");
   if (side != 0 && side != 1) return fail(JFX_ERR_ARG, "side must be 0 (left) or 1 (right)");
+  if (jp->carried[0] || jp->carried[1]) return fail(JFX_ERR_ARG, "this plan kept no row ids (payloads were carried)");
   const u32 *cnt, *pA;
   u64 na;
   if (side == 0) {

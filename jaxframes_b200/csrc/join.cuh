@@ -265,33 +265,113 @@ __device__ __forceinline__ void gather_elem(const void* src, int sdt, u64 n_src,
 
 // Payload columns gathered by the expand kernels as they write each output
 // row (the separate gathers of ParallelSortMergeJoin.join, :1056-1073).
+// A payload is either gathered by row id from its column (src), or was
+// carried through its side's sort as 32-bit words (cw0, and cw1 for an
+// 8-byte dtype) and is read at the row's sorted position, which the expand
+// kernels reach in nearly sequential order.
 constexpr int kMaxJoinPayloads = 8;
 struct JoinPayloads {
   int n;
-  int swap;  // the A side of the expand is the right table
+  int swap;      // the A side of the expand is the right table
+  int gathered;  // some payload is gathered by row id (the kernels need the row ids)
   const void* src[kMaxJoinPayloads];
+  const u32* cw0[kMaxJoinPayloads];  // carried words in sorted order, or null
+  const u32* cw1[kMaxJoinPayloads];
   void* out[kMaxJoinPayloads];
   u64 n_src[kMaxJoinPayloads];
   int sdt[kMaxJoinPayloads], odt[kMaxJoinPayloads];
-  int side[kMaxJoinPayloads];  // 0: gathered by the left row id, 1: by the right row id
+  int side[kMaxJoinPayloads];  // 0: the left table's column, 1: the right table's
+  int kind[kMaxJoinPayloads];  // PayloadKind: the conversion, fixed per column
 };
 
+// Conversions of a payload column, chosen on the host so that the kernels'
+// inner loops carry no per-element dtype dispatch.
+enum PayloadKind : int {
+  PK_GENERIC = 0,  // gather_store
+  PK_SAME4 = 1,    // 4-byte copy (fill: -1 bits, or NaN for float32)
+  PK_SAME8 = 2,    // 8-byte copy (fill: -1 bits, or NaN for float64)
+  PK_I32_F32 = 3,
+  PK_U32_F32 = 4,
+  PK_I64_F32 = 5,
+  PK_U64_F32 = 6,
+};
+inline int payload_kind(int sdt, int odt) {
+  if (sdt == odt) return dtype_size(sdt) == 4 ? PK_SAME4 : dtype_size(sdt) == 8 ? PK_SAME8 : PK_GENERIC;
+  if (odt == JFX_F32) {
+    switch (sdt) {
+      case JFX_I32: return PK_I32_F32;
+      case JFX_U32: return PK_U32_F32;
+      case JFX_I64: return PK_I64_F32;
+      case JFX_U64: return PK_U64_F32;
+    }
+  }
+  return PK_GENERIC;
+}
+
 // Writes every payload of U outputs o[u] (valid when ok[u]); ra / rb are the
-// A / B row ids (-1: none).  Per payload, the U loads go out before the
-// stores (the compiler cannot move loads across stores that may alias).
+// A / B row ids and pa / pb their sorted positions (-1: no row).  Per payload
+// the U loads go out before the stores (the compiler cannot move loads across
+// stores that may alias).
 template <int U>
 __device__ __forceinline__ void write_payloads(const JoinPayloads& p, const u64* o, const bool* ok,
-                                               const long long* ra, const long long* rb) {
+                                               const long long* ra, const long long* rb, const long long* pa,
+                                               const long long* pb) {
   for (int k = 0; k < p.n; ++k) {
-    const bool right = p.side[k] != p.swap;  // row id from the B side
+    const bool right = p.side[k] != p.swap;  // the row comes from the B side
+    const u32* w0 = p.cw0[k];
+    const u32* w1 = p.cw1[k];
     u64 raw[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) raw[u] = ok[u] ? gather_load(p.src[k], p.sdt[k], p.n_src[k], right ? rb[u] : ra[u]) : 0ull;
+    bool valid[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      if (!ok[u]) continue;
-      const long long r = right ? rb[u] : ra[u];
-      gather_store(raw[u], r >= 0 && (u64)r < p.n_src[k], p.sdt[k], p.out[k], p.odt[k], o[u]);
+      const long long r = w0 ? (right ? pb[u] : pa[u]) : (right ? rb[u] : ra[u]);
+      valid[u] = ok[u] && r >= 0 && (w0 || (u64)r < p.n_src[k]);
+      raw[u] = 0ull;
+      if (valid[u]) {
+        if (w0) raw[u] = (u64)w0[r] | (w1 ? (u64)w1[r] << 32 : 0ull);
+        else raw[u] = load_raw(p.src[k], p.sdt[k], (u64)r);
+      }
+    }
+    const float fnan = __int_as_float(0x7fc00000);
+    switch (p.kind[k]) {
+      case PK_SAME4: {
+        const u32 fill = p.odt[k] == JFX_F32 ? 0x7fc00000u : 0xffffffffu;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((u32*)p.out[k])[o[u]] = valid[u] ? (u32)raw[u] : fill;
+        break;
+      }
+      case PK_SAME8: {
+        const u64 fill = p.odt[k] == JFX_F64 ? 0x7ff8000000000000ull : ~0ull;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((u64*)p.out[k])[o[u]] = valid[u] ? raw[u] : fill;
+        break;
+      }
+      case PK_I32_F32:
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((float*)p.out[k])[o[u]] = valid[u] ? (float)(int)raw[u] : fnan;
+        break;
+      case PK_U32_F32:
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((float*)p.out[k])[o[u]] = valid[u] ? (float)(u32)raw[u] : fnan;
+        break;
+      case PK_I64_F32:
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((float*)p.out[k])[o[u]] = valid[u] ? (float)(long long)raw[u] : fnan;
+        break;
+      case PK_U64_F32:
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) ((float*)p.out[k])[o[u]] = valid[u] ? (float)raw[u] : fnan;
+        break;
+      default:
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) gather_store(raw[u], valid[u], p.sdt[k], p.out[k], p.odt[k], o[u]);
     }
   }
 }
@@ -299,12 +379,24 @@ __device__ __forceinline__ void write_payloads(const JoinPayloads& p, const u64*
 // Merged key columns written by the expand kernels (A side's key values).
 struct JoinKeyOut {
   int ncols;
+  int float_key;        // some requested key column is float: written from its original row
+  // one requested 4- or 8-byte integer key column: out = ((packed >> shift) &
+  // mask) + tmin, sign bit flipped back (untransform_int), stored as fast_size bytes
+  int fast_size;
+  u64 fast_flip;
   void* out[kMaxCols];  // per column output, or null
   ColDesc c[kMaxCols];  // A side's columns with the shared packing
 };
 
 template <typename K>
 __device__ __forceinline__ void write_join_key(const JoinKeyOut& ko, u64 o, K packed, u32 row) {
+  if (ko.fast_size) {
+    const ColDesc& c = ko.c[0];
+    const u64 field = (((u64)packed >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull))) + c.tmin;
+    if (ko.fast_size == 8) ((u64*)ko.out[0])[o] = field ^ ko.fast_flip;
+    else ((u32*)ko.out[0])[o] = (u32)field ^ (u32)ko.fast_flip;
+    return;
+  }
   for (int j = 0; j < ko.ncols; ++j) {
     if (!ko.out[j]) continue;
     const ColDesc& c = ko.c[j];
@@ -365,22 +457,25 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_expand_inner(const u64* o
     ii[k] = i0 + r;
     jj[k] = o - OW[r];
   }
+  const bool idx_out = a_out && b_out;
+  const bool rows = idx_out || pay.gathered || ko.float_key;  // row ids needed
   u32 ra[kJoinIPT], lo_k[kJoinIPT];
   K kk[kJoinIPT];
 #pragma unroll
   for (int k = 0; k < kJoinIPT; ++k) {
+    ra[k] = 0xffffffffu;
     if (ob + k >= o1) continue;
-    ra[k] = pA[ii[k]];
+    if (rows) ra[k] = pA[ii[k]];
     lo_k[k] = lo[ii[k]];
     kk[k] = skA[ii[k]];
   }
   int32_t rb[kJoinIPT];
 #pragma unroll
   for (int k = 0; k < kJoinIPT; ++k) {
+    rb[k] = -1;
     if (ob + k >= o1) continue;
-    rb[k] = (int32_t)pB[(u64)lo_k[k] + jj[k]];
+    if (rows) rb[k] = (int32_t)pB[(u64)lo_k[k] + jj[k]];
   }
-  const bool idx_out = a_out && b_out;
   const bool vec = idx_out && ob + kJoinIPT <= o1 &&
                    ((((uintptr_t)(a_out + ob)) | ((uintptr_t)(b_out + ob))) & 15) == 0;
   if (vec) {
@@ -403,15 +498,17 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_expand_inner(const u64* o
   if (pay.n) {
     u64 oo[kJoinIPT];
     bool ok[kJoinIPT];
-    long long la[kJoinIPT], lb[kJoinIPT];
+    long long la[kJoinIPT], lb[kJoinIPT], qa[kJoinIPT], qb[kJoinIPT];
 #pragma unroll
     for (int k = 0; k < kJoinIPT; ++k) {
       oo[k] = ob + k;
       ok[k] = ob + k < o1;
-      la[k] = ok[k] ? (long long)ra[k] : -1;
-      lb[k] = ok[k] ? (long long)rb[k] : -1;
+      la[k] = ok[k] && rows ? (long long)ra[k] : -1;
+      lb[k] = ok[k] && rows ? (long long)rb[k] : -1;
+      qa[k] = ok[k] ? (long long)ii[k] : -1;
+      qb[k] = ok[k] ? (long long)lo_k[k] + (long long)jj[k] : -1;
     }
-    write_payloads<kJoinIPT>(pay, oo, ok, la, lb);
+    write_payloads<kJoinIPT>(pay, oo, ok, la, lb, qa, qb);
   }
 }
 
@@ -425,33 +522,39 @@ __global__ void __launch_bounds__(256) k_join_expand_unique(u64 na, const u32* l
                                                            JoinKeyOut ko, JoinPayloads pay) {
   constexpr int U = 4;
   const u64 stride = (u64)gridDim.x * blockDim.x;
+  const bool rows = a_out || b_out || pay.gathered || ko.float_key;  // row ids needed
   for (u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; i0 < na; i0 += stride * U) {
     u32 ra[U], l[U];
     K kk[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const u64 i = i0 + (u64)u * stride;
+      ra[u] = 0xffffffffu;
       if (i < na) {
-        ra[u] = pA[i];
+        if (rows) ra[u] = pA[i];
         l[u] = lo[i];
         kk[u] = skA[i];
       }
     }
     u32 rb[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (i0 + (u64)u * stride < na) rb[u] = pB[l[u]];
+    for (int u = 0; u < U; ++u) {
+      rb[u] = 0xffffffffu;
+      if (rows && i0 + (u64)u * stride < na) rb[u] = pB[l[u]];
+    }
     u64 oo[U];
     bool ok[U];
-    long long la[U], lb[U];
+    long long la[U], lb[U], qa[U], qb[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       oo[u] = i0 + (u64)u * stride;
       ok[u] = oo[u] < na;
-      la[u] = ok[u] ? (long long)ra[u] : -1;
-      lb[u] = ok[u] ? (long long)rb[u] : -1;
+      la[u] = ok[u] && rows ? (long long)ra[u] : -1;
+      lb[u] = ok[u] && rows ? (long long)rb[u] : -1;
+      qa[u] = ok[u] ? (long long)oo[u] : -1;
+      qb[u] = ok[u] ? (long long)l[u] : -1;
     }
-    if (pay.n) write_payloads<U>(pay, oo, ok, la, lb);
+    if (pay.n) write_payloads<U>(pay, oo, ok, la, lb, qa, qb);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!ok[u]) break;
@@ -469,17 +572,20 @@ __global__ void __launch_bounds__(256) k_join_expand_first(u64 na, const u32* lo
                                                           const u32* pA, const u32* pB, const K* skA,
                                                           int32_t* a_out, int32_t* b_out, JoinKeyOut ko,
                                                           JoinPayloads pay) {
+  const bool rows = a_out || b_out || pay.gathered || ko.float_key;  // row ids needed
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (u64)gridDim.x * blockDim.x) {
-    const u32 ra = pA[i];
-    const int32_t rb = cnt[i] ? (int32_t)pB[lo[i]] : -1;
+    const u32 c = cnt[i], l = lo[i];
+    const u32 ra = rows ? pA[i] : 0xffffffffu;
+    const int32_t rb = c ? (rows ? (int32_t)pB[l] : 0) : -1;
     if (a_out) a_out[i] = (int32_t)ra;
     if (b_out) b_out[i] = rb;
     write_join_key<K>(ko, i, skA[i], ra);
     if (pay.n) {
       const u64 oo[1] = {i};
       const bool ok[1] = {true};
-      const long long la[1] = {(long long)ra}, lb[1] = {(long long)rb};
-      write_payloads<1>(pay, oo, ok, la, lb);
+      const long long la[1] = {rows ? (long long)ra : -1}, lb[1] = {rows ? (long long)rb : -1};
+      const long long qa[1] = {(long long)i}, qb[1] = {c ? (long long)l : -1};
+      write_payloads<1>(pay, oo, ok, la, lb, qa, qb);
     }
   }
 }

@@ -788,6 +788,10 @@ struct HistIntArgs {
   int kshift, npass;
   int shift[8];
   u32 mask[8];
+  // optional: the first pass's digit counts of every radix tile, digit-major
+  // [RADIX][tiles], so that pass can run in two phases as well
+  u32* tile_counts;
+  u64 tiles;
 };
 
 template <typename K, typename T, int RB>
@@ -795,9 +799,47 @@ __global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
   constexpr int RADIX = 1 << RB;
   extern __shared__ u32 sh[];
   const int total = a.npass * RADIX;
+  const T* col = (const T*)a.col;
+  if (a.tile_counts) {
+    // tile by tile (the radix pass's tiles): all passes' counts plus the
+    // first pass's counts of this tile
+    constexpr int TILE = PassLayout<K, RB>::TILE, IPT = TILE / 256;
+    u32* tsh = sh + total;
+    for (int i = threadIdx.x; i < total + RADIX; i += blockDim.x) sh[i] = 0u;
+    __syncthreads();
+    for (u64 t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+      const u64 base = t * TILE;
+      const u32 tn = (u32)min((u64)TILE, a.n - base);
+      T raw[IPT];
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        const u32 r = i * 256 + threadIdx.x;
+        raw[i] = r < tn ? __ldg(col + base + r) : (T)0;
+      }
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        if (i * 256 + threadIdx.x >= tn) break;
+        const K k = (K)((((u64)raw[i] ^ a.flip) - a.tmin) << a.kshift);
+        atomicAdd(&tsh[(u32)(k >> a.shift[0]) & a.mask[0]], 1u);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+          if (p >= a.npass) break;
+          atomicAdd(&sh[p * RADIX + ((u32)(k >> a.shift[p]) & a.mask[p])], 1u);
+        }
+      }
+      __syncthreads();
+      for (int d = threadIdx.x; d < RADIX; d += blockDim.x) {
+        a.tile_counts[(u64)d * a.tiles + t] = tsh[d];
+        tsh[d] = 0u;
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < total; i += blockDim.x)
+      if (sh[i]) atomicAdd(&a.hist[i], sh[i]);
+    return;
+  }
   for (int i = threadIdx.x; i < total; i += blockDim.x) sh[i] = 0u;
   __syncthreads();
-  const T* col = (const T*)a.col;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   constexpr int U = 8;  // rows per thread per step, loads issued together
   for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < a.n; r0 += stride * U) {
@@ -1288,6 +1330,17 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   const u64 tiles = (u64)ceil_div(n, PassLayout<K, RB>::TILE);
   JFX_CUDA(cudaMemsetAsync(b.status[0], 0, tiles * RADIX * sizeof(u32), s));
 
+  // the passes after the first of a plain digit sort run in two phases (no
+  // look-back); the first pass too when the histogram kernel can count its
+  // tiles (one plain integer key column)
+  const bool two_phase = rq.digit_mode == DIG_BITS && g_tuning.two_phase && tiles >= 2;
+  const int d0 = rq.pack.c[0].dtype;
+  const bool int_key = rq.pack.ncols == 1 && rq.key_mode == KEY_PACK && rq.digit_mode == DIG_BITS &&
+                       !rq.targets && !(rq.pack.c[0].flags & CF_DESC) &&
+                       (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
+  // (a gathered first pass reads its tiles in another order than the column)
+  const bool first_two_phase = two_phase && int_key && !rq.gather_idx;
+
   HistArgs h;
   memset(&h, 0, sizeof h);
   h.pack = rq.pack;
@@ -1309,14 +1362,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     static bool attr = false;
     if (!attr) {
       JFX_CUDA(cudaFuncSetAttribute(k_hist<K, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
-      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u64, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
-      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u32, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
+      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u64, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
+      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u32, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
       attr = true;
     }
-    const int d0 = rq.pack.c[0].dtype;
-    const bool int_key = rq.pack.ncols == 1 && rq.key_mode == KEY_PACK && rq.digit_mode == DIG_BITS &&
-                         !rq.targets && !(rq.pack.c[0].flags & CF_DESC) &&
-                         (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
     if (int_key) {
       HistIntArgs hi;
       memset(&hi, 0, sizeof hi);
@@ -1331,10 +1380,18 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
         hi.shift[p] = shift[p];
         hi.mask[p] = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
       }
+      int g = std::max(grid, 1);
+      size_t sm = smem;
+      if (first_two_phase) {
+        hi.tile_counts = b.status[1];
+        hi.tiles = tiles;
+        g = (int)std::min<u64>(tiles, (u64)device_sm_count() * 8);
+        sm += (size_t)RADIX * sizeof(u32);
+      }
       if (d0 == JFX_I64 || d0 == JFX_U64)
-        k_hist_int<K, u64, RB><<<std::max(grid, 1), 256, smem, s>>>(hi), note_launch();
+        k_hist_int<K, u64, RB><<<g, 256, sm, s>>>(hi), note_launch();
       else
-        k_hist_int<K, u32, RB><<<std::max(grid, 1), 256, smem, s>>>(hi), note_launch();
+        k_hist_int<K, u32, RB><<<g, 256, sm, s>>>(hi), note_launch();
     } else {
       k_hist<K, RB><<<std::max(grid, 1), 256, smem, s>>>(h), note_launch();
     }
@@ -1343,8 +1400,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
   JFX_CUDA(cudaGetLastError());
 
-  // later passes of a plain digit sort run in two phases (no look-back)
-  const bool two_phase = rq.digit_mode == DIG_BITS && g_tuning.two_phase && tiles >= 2;
+  if (first_two_phase) {
+    k_tile_scan<RB><<<RADIX, 256, 0, s>>>(b.status[1], tiles, b.base, b.status[0]), note_launch();
+    JFX_CUDA(cudaGetLastError());
+  }
   u32* out_vals[kMaxWords];
   for (int w = 0; w < kMaxWords; ++w) out_vals[w] = rq.vout_final[w];
   if (!out_vals[0]) out_vals[0] = rq.perm_out;
@@ -1396,6 +1455,11 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       a.status_next = nullptr;
     }
     if (two_phase && p == 0) a.status_next = nullptr;
+    if (first_two_phase && p == 0) {
+      a.tile_base = b.status[0];
+      a.ntiles = tiles;
+      a.status = nullptr;
+    }
     if (p == 0) {
       JFX_TRY((launch_pass<K, RB, true, NW>(a, n, s)));
     } else {

@@ -373,9 +373,19 @@ class SortBasedGroupBy:
         return dict(zip(key_names, uniq)), out
 
 
-def _join_prepare(lcols, rcols, how: str):
-    """jfx_join_prepare: returns (plan, num_out, workspace); the workspace must
-    outlive every later call that uses the plan."""
+def _payload_array(payloads, outs=None):
+    arr = (_lib.JoinPayload * max(len(payloads), 1))()
+    for k, (name, t, side, odt) in enumerate(payloads):
+        arr[k] = _lib.JoinPayload(t.data_ptr() if t.numel() else None, t.numel(), _lib.jfx_dtype(t), side,
+                                  outs[name].data_ptr() if outs is not None else None, _lib.TORCH_TO_JFX[odt], 0)
+    return arr
+
+
+def _join_prepare(lcols, rcols, how: str, payloads=None):
+    """jfx_join_prepare (or jfx_join_prepare_payloads when the payload columns
+    [(name, tensor, side, out dtype)] are given, at most 8): returns (plan,
+    num_out, workspace); the workspace must outlive every later call that
+    uses the plan."""
     L = _lib.lib()
     nl, nr = lcols[0].numel(), rcols[0].numel()
     ws = _lib.workspace(_lib.WS_JOIN, nl, nr, device=lcols[0].device)
@@ -383,8 +393,13 @@ def _join_prepare(lcols, rcols, how: str):
     m = ctypes.c_int64(0)
     la = (_lib.Column * len(lcols))(*[_lib.column(c) for c in lcols])
     ra = (_lib.Column * len(rcols))(*[_lib.column(c) for c in rcols])
-    check(L.jfx_join_prepare(la, nl, ra, nr, len(lcols), _lib.JOIN_KINDS[how], ctypes.byref(plan), ctypes.byref(m),
-                             ws.data_ptr(), ws.numel(), _stream()))
+    if payloads:
+        check(L.jfx_join_prepare_payloads(la, nl, ra, nr, len(lcols), _lib.JOIN_KINDS[how], _payload_array(payloads),
+                                          len(payloads), ctypes.byref(plan), ctypes.byref(m), ws.data_ptr(),
+                                          ws.numel(), _stream()))
+    else:
+        check(L.jfx_join_prepare(la, nl, ra, nr, len(lcols), _lib.JOIN_KINDS[how], ctypes.byref(plan),
+                                 ctypes.byref(m), ws.data_ptr(), ws.numel(), _stream()))
     return plan, m.value, ws
 
 
@@ -408,23 +423,10 @@ def _join_expand_gather(plan, m, like, key_col, payloads):
     if m:
         chunks = [payloads[i:i + 8] for i in range(0, len(payloads), 8)] or [[]]
         for ci, chunk in enumerate(chunks):
-            arr = (_lib.JoinPayload * max(len(chunk), 1))()
-            for k, (name, t, side, odt) in enumerate(chunk):
-                arr[k] = _lib.JoinPayload(t.data_ptr() if t.numel() else None, t.numel(), _lib.jfx_dtype(t), side,
-                                          outs[name].data_ptr(), _lib.TORCH_TO_JFX[odt], 0)
             keys = (ctypes.c_void_p * 1)(mk.data_ptr()) if ci == 0 else None
-            check(L.jfx_join_expand_gather(ctypes.byref(plan), None, None, keys, arr, len(chunk), _stream()))
+            check(L.jfx_join_expand_gather(ctypes.byref(plan), None, None, keys, _payload_array(chunk, outs),
+                                           len(chunk), _stream()))
     return mk, outs
-
-
-_SIDE_STREAMS = {}
-
-
-def _side_stream(dev):
-    s = _SIDE_STREAMS.get(dev)
-    if s is None:
-        s = _SIDE_STREAMS[dev] = torch.cuda.Stream(device=dev)
-    return s
 
 
 def _join_unmatched(plan, side: int, n: int, like):
@@ -516,27 +518,19 @@ class ParallelSortMergeJoin:
                 t = as_device(a)
                 out[f"right_{c}"] = _gather(t, ri, t.dtype if _is_float(t) else config.default_float())
             return mk, out
-        # keys first; host payload columns are copied on a side stream while
-        # the keys are sorted, and gathered inside the expand kernel
+        # the payload columns are handed to the prepare step, which carries
+        # them through the sorts when they fit (8 at most per call), and are
+        # written by the expand kernel
         lk, rk = as_device(left_keys), as_device(right_keys)
-        cur = torch.cuda.current_stream(lk.device)
-        side = _side_stream(lk.device)
-        side.wait_stream(cur)
-        with torch.cuda.stream(side):
-            lv = {c: as_device(a, lk.device) for c, a in left_values.items()}
-            rv = {c: as_device(a, lk.device) for c, a in right_values.items()}
-        ready = torch.cuda.Event()
-        ready.record(side)
-        (lk,), (rk,) = _same_dtypes([lk], [rk])
-        plan, m, ws = _join_prepare([lk], [rk], how)
-        cur.wait_event(ready)
         payloads = []
-        for c, t in lv.items():
-            t.record_stream(cur)
+        for c, a in left_values.items():
+            t = as_device(a, lk.device)
             payloads.append((f"left_{c}", t, 0, t.dtype if _is_float(t) else config.default_float()))
-        for c, t in rv.items():
-            t.record_stream(cur)
+        for c, a in right_values.items():
+            t = as_device(a, lk.device)
             payloads.append((f"right_{c}", t, 1, t.dtype if _is_float(t) else config.default_float()))
+        (lk,), (rk,) = _same_dtypes([lk], [rk])
+        plan, m, ws = _join_prepare([lk], [rk], how, payloads if 0 < len(payloads) <= 8 else None)
         mk, out = _join_expand_gather(plan, m, lk, rk if how == "right" else lk, payloads)
         del ws
         return mk, out

@@ -318,6 +318,32 @@ def test_join_many_payloads_partial_matches(P, how):
         np.testing.assert_array_equal(g, eout[c], err_msg=f"{how} {c}")
 
 
+@pytest.mark.parametrize("how", ["inner", "left", "right"])
+@pytest.mark.parametrize("layout", ["both_carried", "right_too_wide", "float_key"])
+def test_join_carried_payloads(P, how, layout):
+    """Payload columns carried through the sorts (4- and 8-byte words, at most
+    4 per side) or gathered when a side does not fit or the key is float;
+    duplicate keys on both sides, unmatched rows on both sides."""
+    rng = np.random.default_rng(3 + len(how) + len(layout))
+    nl, nr = 40_000, 25_000
+    kdt = np.float32 if layout == "float_key" else np.int64
+    lk = rng.integers(0, 20_000, nl).astype(kdt)
+    rk = rng.integers(5_000, 30_000, nr).astype(kdt)
+    lv = {"a": rng.standard_normal(nl), "b": rng.integers(-9, 9, nl).astype(np.int32)}
+    rv = {"c": rng.integers(-2**40, 2**40, nr), "d": rng.standard_normal(nr).astype(np.float32)}
+    if layout == "right_too_wide":
+        rv["e"] = rng.integers(0, 99, nr).astype(np.int64)
+        rv["f"] = rng.integers(0, 99, nr).astype(np.uint64)
+    mk, out = P.sort_merge_join(lk, lv, rk, rv, how)
+    emk, eout, _, _ = O.sort_merge_join(lk, lv, rk, rv, how)
+    np.testing.assert_array_equal(_np(mk), emk)
+    assert set(out) == set(eout)
+    for c in eout:
+        g = _np(out[c])
+        assert g.dtype == eout[c].dtype, c
+        np.testing.assert_array_equal(g, eout[c], err_msg=f"{how} {layout} {c}")
+
+
 @pytest.mark.parametrize("how", ["left", "right", "outer"])
 def test_non_inner_joins(P, how):
     rng = np.random.default_rng(len(how))
