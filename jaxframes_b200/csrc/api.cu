@@ -1448,7 +1448,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   a.status_next = bb.status[1];
   a.tile_counter = bb.counters;
   a.seg.pass_index = 0;
-  JFX_TRY((launch_pass<u32, RB, true>(a, (u64)n, s, bb.max_tiles)));
+  JFX_TRY((launch_pass<u32, RB, 2>(a, (u64)n, s, bb.max_tiles)));
   {
     const u64 tot = (u64)nq * (num_partitions + 1);
     k_part_offsets<<<grid_for(tot, 256), 256, 0, s>>>(bb.row_base, bb.base, (u32)nq, npass, RADIX,
@@ -1474,7 +1474,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
     b.tile_counter = bb.counters + p;
     b.seg.pass_index = p;
     b.seg.key_shift_q = last ? key_bits : 0;
-    JFX_TRY((launch_pass<u32, RB, false>(b, (u64)n, s, bb.max_tiles)));
+    JFX_TRY((launch_pass<u32, RB, 0>(b, (u64)n, s, bb.max_tiles)));
     kin = (const u32*)b.keys_out;
     vin = b.vout[0];
   }

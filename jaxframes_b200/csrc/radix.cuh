@@ -340,8 +340,13 @@ __device__ __forceinline__ K pack2(const PackDesc& pd, u64 r0, u64 r1) {
   return k;
 }
 
-template <typename K, int RB, bool FIRST, int NW>
+// FM: 0 = a later pass (keys and payload words from the previous pass);
+// 1 = the first pass over one plain 32/64-bit integer key column (a lean
+// instantiation: fewer registers, more CTAs per SM); 2 = any other first pass
+// (packed or hashed columns, gathered rows, the learned position).
+template <typename K, int RB, int FM, int NW>
 __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
+  constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
   constexpr int THREADS = L::THREADS, IPT = L::IPT, RADIX = L::RADIX, WARPS = L::WARPS,
                 TILE = L::TILE;
@@ -422,38 +427,56 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
   // tile is issued before any is used (one DRAM round trip per tile).
   K key[IPT];
   u32 rd[IPT];
-  // first pass over one plain 32/64-bit integer column (the common key):
-  // the dtype dispatch happens once per tile, not per item
-  const int d0 = a.pack.c[0].dtype;
-  const bool int_first = FIRST && full && simple_first && a.pack.ncols == 1 && a.key_mode == KEY_PACK &&
-                         a.digit_mode == DIG_BITS && !(a.pack.c[0].flags & CF_DESC) &&
-                         (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
   if (!FIRST && full && a.digit_mode == DIG_BITS) {
     const K* kin = (const K*)a.keys_in + base + toff;
 #pragma unroll
     for (int i = 0; i < IPT; ++i) key[i] = kin[i * 32];
 #pragma unroll
     for (int i = 0; i < IPT; ++i) rd[i] = (u32)(key[i] >> a.shift) & mask;
-  } else if (int_first) {
-    u64 raw[IPT];
-    if (d0 == JFX_I64 || d0 == JFX_U64) {
+  } else if constexpr (FM == 1) {
+    // first pass over one or two plain integer columns of one width: the
+    // dtype is dispatched once per tile; each transform is the sign flip
+    const int d0 = a.pack.c[0].dtype;
+    const bool two = a.pack.ncols == 2;
+    const u64 flip0 = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
+    const int d1 = two ? a.pack.c[1].dtype : d0;
+    const u64 flip1 = d1 == JFX_I64 ? 0x8000000000000000ull : d1 == JFX_I32 ? 0x80000000ull : 0ull;
+    const u64 tmin0 = a.pack.c[0].tmin, tmin1 = two ? a.pack.c[1].tmin : 0ull;
+    const int sh0 = a.pack.c[0].shift, sh1 = two ? a.pack.c[1].shift : 0;
+    const bool b1 = two && a.pack.c[1].bits;  // a constant second column adds nothing
+    if (dtype_size(d0) == 8) {
       const u64* src = (const u64*)a.pack.c[0].ptr + base + toff;
+      u64 raw[IPT];
 #pragma unroll
-      for (int i = 0; i < IPT; ++i) raw[i] = __ldg(src + i * 32);
+      for (int i = 0; i < IPT; ++i) raw[i] = (full || toff + i * 32 < tile_n) ? __ldg(src + i * 32) : 0ull;
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) key[i] = (K)(((raw[i] ^ flip0) - tmin0) << sh0);
+      if (b1) {
+        const u64* src1 = (const u64*)a.pack.c[1].ptr + base + toff;
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) raw[i] = (full || toff + i * 32 < tile_n) ? __ldg(src1 + i * 32) : 0ull;
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) key[i] |= (K)(((raw[i] ^ flip1) - tmin1) << sh1);
+      }
     } else {
       const u32* src = (const u32*)a.pack.c[0].ptr + base + toff;
+      const u32* src1 = (const u32*)(b1 ? a.pack.c[1].ptr : a.pack.c[0].ptr) + base + toff;
+      u32 r0[IPT], r1[IPT];
 #pragma unroll
-      for (int i = 0; i < IPT; ++i) raw[i] = __ldg(src + i * 32);
-    }
-    // order-preserving transform of transform_raw for these types: flip the sign bit
-    const u64 flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
-    const u64 tmin = a.pack.c[0].tmin;
-    const int kshift = a.pack.c[0].shift;
+      for (int i = 0; i < IPT; ++i) {
+        const bool in = full || toff + i * 32 < tile_n;
+        r0[i] = in ? __ldg(src + i * 32) : 0u;
+        r1[i] = (in && b1) ? __ldg(src1 + i * 32) : 0u;
+      }
 #pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-      key[i] = (K)(((raw[i] ^ flip) - tmin) << kshift);
-      rd[i] = (u32)(key[i] >> a.shift) & mask;
+      for (int i = 0; i < IPT; ++i) {
+        key[i] = (K)((((u64)r0[i] ^ flip0) - tmin0) << sh0);
+        if (b1) key[i] |= (K)((((u64)r1[i] ^ flip1) - tmin1) << sh1);
+      }
     }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i)
+      rd[i] = (full || toff + i * 32 < tile_n) ? (u32)(key[i] >> a.shift) & mask : (u32)RADIX;
   } else if (two_first) {
     // two key columns: both columns' loads for 8 items, then pack
 #pragma unroll
@@ -782,10 +805,12 @@ __global__ void __launch_bounds__(256) k_hist(HistArgs a) {
 // a subtraction and one shared-memory atomic per pass.
 struct HistIntArgs {
   const void* col;
+  const void* col2;  // optional second key column (same storage type), less significant
   u32* hist;  // [npass][RADIX], zeroed
   u64 n;
   u64 flip, tmin;
-  int kshift, npass;
+  u64 flip2, tmin2;
+  int kshift, kshift2, npass;
   int shift[8];
   u32 mask[8];
   // optional: the first pass's digit counts of every radix tile, digit-major
@@ -800,6 +825,7 @@ __global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
   extern __shared__ u32 sh[];
   const int total = a.npass * RADIX;
   const T* col = (const T*)a.col;
+  const T* col2 = (const T*)a.col2;
   if (a.tile_counts) {
     // tile by tile (the radix pass's tiles): all passes' counts plus the
     // first pass's counts of this tile
@@ -810,16 +836,18 @@ __global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
     for (u64 t = blockIdx.x; t < a.tiles; t += gridDim.x) {
       const u64 base = t * TILE;
       const u32 tn = (u32)min((u64)TILE, a.n - base);
-      T raw[IPT];
+      T raw[IPT], raw2[IPT];
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
         const u32 r = i * 256 + threadIdx.x;
         raw[i] = r < tn ? __ldg(col + base + r) : (T)0;
+        raw2[i] = (col2 && r < tn) ? __ldg(col2 + base + r) : (T)0;
       }
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
         if (i * 256 + threadIdx.x >= tn) break;
-        const K k = (K)((((u64)raw[i] ^ a.flip) - a.tmin) << a.kshift);
+        K k = (K)((((u64)raw[i] ^ a.flip) - a.tmin) << a.kshift);
+        if (col2) k |= (K)((((u64)raw2[i] ^ a.flip2) - a.tmin2) << a.kshift2);
         atomicAdd(&tsh[(u32)(k >> a.shift[0]) & a.mask[0]], 1u);
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
@@ -843,16 +871,18 @@ __global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
   const u64 stride = (u64)gridDim.x * blockDim.x;
   constexpr int U = 8;  // rows per thread per step, loads issued together
   for (u64 r0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; r0 < a.n; r0 += stride * U) {
-    T raw[U];
+    T raw[U], raw2[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const u64 r = r0 + (u64)u * stride;
       raw[u] = r < a.n ? __ldg(col + r) : (T)0;
+      raw2[u] = (col2 && r < a.n) ? __ldg(col2 + r) : (T)0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (r0 + (u64)u * stride >= a.n) break;
-      const K k = (K)((((u64)raw[u] ^ a.flip) - a.tmin) << a.kshift);
+      K k = (K)((((u64)raw[u] ^ a.flip) - a.tmin) << a.kshift);
+      if (col2) k |= (K)((((u64)raw2[u] ^ a.flip2) - a.tmin2) << a.kshift2);
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
         if (p >= a.npass) break;
@@ -1158,11 +1188,25 @@ inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s
     const bool int_key = pd.ncols == 1 && !(pd.c[0].flags & CF_DESC) &&
                          (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
     const u64 flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
+    bool all_int = true;  // every column a plain integer one: one specialised launch per column
+    for (int j = 0; j < pd.ncols; ++j) {
+      const int dt = pd.c[j].dtype;
+      all_int &= !(pd.c[j].flags & CF_DESC) && (dt == JFX_I32 || dt == JFX_I64 || dt == JFX_U32 || dt == JFX_U64);
+    }
     if (int_key && (d0 == JFX_I64 || d0 == JFX_U64))
       k_minmax_int<u64><<<grid, 256, 0, s>>>((const u64*)pd.c[0].ptr, n, flip, dev_out), note_launch();
     else if (int_key)
       k_minmax_int<u32><<<grid, 256, 0, s>>>((const u32*)pd.c[0].ptr, n, flip, dev_out), note_launch();
-    else
+    else if (all_int && pd.ncols <= 4) {
+      for (int j = 0; j < pd.ncols; ++j) {
+        const int dt = pd.c[j].dtype;
+        const u64 fj = dt == JFX_I64 ? 0x8000000000000000ull : dt == JFX_I32 ? 0x80000000ull : 0ull;
+        if (dtype_size(dt) == 8)
+          k_minmax_int<u64><<<grid, 256, 0, s>>>((const u64*)pd.c[j].ptr, n, fj, dev_out + 2 * j), note_launch();
+        else
+          k_minmax_int<u32><<<grid, 256, 0, s>>>((const u32*)pd.c[j].ptr, n, fj, dev_out + 2 * j), note_launch();
+      }
+    } else
       k_minmax<<<grid, 256, 0, s>>>(pd, n, dev_out), note_launch();
   }
   JFX_CUDA(cudaGetLastError());
@@ -1250,18 +1294,19 @@ inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b, int words = 1) {
   b.status[1] = ar.take<u32>(b.status_words);
 }
 
-template <typename K, int RB, bool FIRST, int NW = 1>
+template <typename K, int RB, int FM, int NW = 1>
 inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles = 0) {
+  constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FIRST, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FM, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::SMEM));
     attr_set = true;
   }
   int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
   const long t = timing_begin(s);
-  k_onesweep<K, RB, FIRST, NW><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
+  k_onesweep<K, RB, FM, NW><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
   if (t >= 0) {
     // algorithmic bytes: the first pass reads the key columns and writes
     // key + row id; later passes read and write key + row id
@@ -1334,12 +1379,18 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   // look-back); the first pass too when the histogram kernel can count its
   // tiles (one plain integer key column)
   const bool two_phase = rq.digit_mode == DIG_BITS && g_tuning.two_phase && tiles >= 2;
-  const int d0 = rq.pack.c[0].dtype;
-  const bool int_key = rq.pack.ncols == 1 && rq.key_mode == KEY_PACK && rq.digit_mode == DIG_BITS &&
-                       !rq.targets && !(rq.pack.c[0].flags & CF_DESC) &&
-                       (d0 == JFX_I32 || d0 == JFX_I64 || d0 == JFX_U32 || d0 == JFX_U64);
+  const int d0 = rq.pack.c[0].dtype, d1 = rq.pack.ncols > 1 ? rq.pack.c[1].dtype : 0;
+  auto plain_int = [](int dt) { return dt == JFX_I32 || dt == JFX_I64 || dt == JFX_U32 || dt == JFX_U64; };
+  // one plain integer key column, or two of the same width
+  const bool int_key = (rq.pack.ncols == 1 || (rq.pack.ncols == 2 && plain_int(d1) && dtype_size(d1) == dtype_size(d0) &&
+                                               !(rq.pack.c[1].flags & CF_DESC))) &&
+                       rq.key_mode == KEY_PACK && rq.digit_mode == DIG_BITS && !rq.targets &&
+                       !(rq.pack.c[0].flags & CF_DESC) && plain_int(d0);
   // (a gathered first pass reads its tiles in another order than the column)
   const bool first_two_phase = two_phase && int_key && !rq.gather_idx;
+  // the first pass's lean instantiation: one or two plain integer columns of
+  // one width, read in order
+  const bool int1 = int_key && !rq.gather_idx;
 
   HistArgs h;
   memset(&h, 0, sizeof h);
@@ -1375,6 +1426,12 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       hi.flip = d0 == JFX_I64 ? 0x8000000000000000ull : d0 == JFX_I32 ? 0x80000000ull : 0ull;
       hi.tmin = rq.pack.c[0].tmin;
       hi.kshift = rq.pack.c[0].shift;
+      if (rq.pack.ncols == 2) {
+        hi.col2 = rq.pack.c[1].ptr;
+        hi.flip2 = d1 == JFX_I64 ? 0x8000000000000000ull : d1 == JFX_I32 ? 0x80000000ull : 0ull;
+        hi.tmin2 = rq.pack.c[1].tmin;
+        hi.kshift2 = rq.pack.c[1].shift;
+      }
       hi.npass = npass;
       for (int p = 0; p < 8; ++p) {
         hi.shift[p] = shift[p];
@@ -1460,10 +1517,12 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       a.ntiles = tiles;
       a.status = nullptr;
     }
-    if (p == 0) {
-      JFX_TRY((launch_pass<K, RB, true, NW>(a, n, s)));
+    if (p == 0 && int1) {
+      JFX_TRY((launch_pass<K, RB, 1, NW>(a, n, s)));
+    } else if (p == 0) {
+      JFX_TRY((launch_pass<K, RB, 2, NW>(a, n, s)));
     } else {
-      JFX_TRY((launch_pass<K, RB, false, NW>(a, n, s)));
+      JFX_TRY((launch_pass<K, RB, 0, NW>(a, n, s)));
     }
   }
   rq.keys_result = out_keys;
