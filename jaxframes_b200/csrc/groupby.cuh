@@ -332,135 +332,187 @@ __device__ __forceinline__ void slot_store(const GroupArgs& a, int c, u64 slot, 
   }
 }
 
-// Segmented reduction of one value column over the warp's rows.
+// The value of sorted row `pos` (carried columns: lo/hi words already read).
 template <int KIND>
-__device__ __forceinline__ void reduce_column(const GroupArgs& a, int c, const u32 (&fm)[kGroupIPT],
-                                              const u32 (&pr)[kGroupIPT], u64 w, u64 wbeg, u64 wend,
-                                              u32 gbase, bool closed_end) {
+__device__ __forceinline__ u64 carried_word(const ValDesc& v, u32 lo, u32 hi) {
+  if (dtype_size(v.dtype) == 8) return (u64)lo | ((u64)hi << 32);
+  if (KIND == VK_F) return __double_as_longlong((double)__uint_as_float(lo));
+  if (KIND == VK_I) return (u64)(long long)(int)lo;
+  return (u64)lo;
+}
+
+// One value column over the warp's rows, lane-sequential: lane l owns the
+// kGroupIPT consecutive rows r0.. (bit j of fl: row r0+j starts a group).
+// Pass 1 folds each lane's rows after its last group start; a segmented
+// scan across the 32 lanes gives every lane the part of its first group that
+// lies in earlier lanes; pass 2 walks the lane's rows again and writes each
+// group where it ends.  Groups that begin in an earlier warp or run past the
+// warp end leave slot records for k_group_fixup, as before.
+template <int KIND>
+__device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u64 w, u64 r0, int nv, u32 fl,
+                                                   u32 gfirst, bool last_lane, bool end_closes, bool next_flag,
+                                                   const u32 (&pr)[kGroupIPT]) {
   const ValDesc& v = a.v[c];
   const int lane = threadIdx.x & 31;
   const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
-  const u32 le = (2u << lane) - 1u;  // lanemask_le
-  Agg<KIND> open = agg_identity<KIND>();
-  bool open_valid = false, open_started = false;
-  u32 open_gid = 0, gcount = 0;
-  // issue every gather of the warp's rows before the scan (memory-level parallelism)
   u64 word[kGroupIPT];
+  if (need_vals) {
+    if (v.carried) {
+      u32 lo[kGroupIPT], hi[kGroupIPT];
+      const bool wide = dtype_size(v.dtype) == 8;
+      if (nv == kGroupIPT) {
 #pragma unroll
-  for (int s = 0; s < kGroupIPT; ++s) {
-    const u64 row = wbeg + (u64)s * 32 + lane;
-    word[s] = (need_vals && row < wend) ? value_word<KIND>(v, pr[s]) : 0ull;
-  }
+        for (int q = 0; q < kGroupIPT / 4; ++q) {
+          reinterpret_cast<uint4*>(lo)[q] = __ldg(reinterpret_cast<const uint4*>((const u32*)v.ptr + r0) + q);
+          if (wide) reinterpret_cast<uint4*>(hi)[q] = __ldg(reinterpret_cast<const uint4*>((const u32*)v.ptr_hi + r0) + q);
+        }
+      } else {
 #pragma unroll
-  for (int s = 0; s < kGroupIPT; ++s) {
-    const u64 step0 = wbeg + (u64)s * 32;
-    if (step0 >= wend) break;
-    const u64 row = step0 + lane;
-    const bool valid = row < wend;
-    const u32 f = fm[s];
-    Agg<KIND> st = agg_identity<KIND>();
-    if (valid) {
-      st.cnt = 1;
-      if (need_vals) st.sum = st.mn = st.mx = word[s];
-    }
-    const u32 hb = f & le;
-    const int h = hb ? 31 - __clz(hb) : -1;
-    const int lo = h < 0 ? 0 : h;
+        for (int j = 0; j < kGroupIPT; ++j) {
+          lo[j] = j < nv ? __ldg((const u32*)v.ptr + r0 + j) : 0u;
+          hi[j] = (wide && j < nv) ? __ldg((const u32*)v.ptr_hi + r0 + j) : 0u;
+        }
+      }
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      Agg<KIND> up = agg_shfl_up<KIND>(st, o);
-      if (lane - o >= lo) st = agg_combine<KIND>(up, st);
-    }
-    Agg<KIND> full = st;
-    bool started = h >= 0;
-    if (h < 0) {
-      if (open_valid) full = agg_combine<KIND>(open, st);
-      started = open_valid && open_started;
-    }
-    const u32 gid = gbase + gcount + __popc(f & le) - 1u;
-    const bool next_in_step = valid && lane < 31 && (row + 1 < wend);
-    const bool last_in_step = valid && !next_in_step;
-    bool closes;
-    if (next_in_step) closes = (f >> (lane + 1)) & 1u;
-    else if (row + 1 < wend) closes = (s + 1 < kGroupIPT) ? (fm[s + 1] & 1u) : true;
-    else closes = closed_end;
-    if (valid && (closes && (next_in_step || last_in_step))) {
-      if (started) agg_finalize<KIND>(v, gid, full);
-      else slot_store<KIND>(a, c, 2 * w, gid, 0u, full);  // the warp's first group, begun earlier
-    }
-    const u32 vm = __ballot_sync(0xffffffffu, valid);
-    const int last = 31 - __clz(vm);
-    const bool lc = __shfl_sync(0xffffffffu, closes, last);
-    Agg<KIND> lf = agg_shfl<KIND>(full, last);
-    const bool ls = __shfl_sync(0xffffffffu, started, last);
-    const u32 lg = __shfl_sync(0xffffffffu, gid, last);
-    if (lc) {
-      open_valid = false;
+      for (int j = 0; j < kGroupIPT; ++j) word[j] = carried_word<KIND>(v, lo[j], wide ? hi[j] : 0u);
     } else {
-      open = lf;
-      open_valid = true;
-      open_started = ls;
-      open_gid = lg;
+#pragma unroll
+      for (int j = 0; j < kGroupIPT; ++j) word[j] = j < nv ? value_word<KIND>(v, pr[j]) : 0ull;
     }
-    gcount += __popc(f);
   }
-  if (open_valid && lane == 0) slot_store<KIND>(a, c, 2 * w + 1, open_gid, open_started ? 1u : 0u, open);
+  // pass 1: the lane's rows after its last group start (all rows without one)
+  Agg<KIND> tail = agg_identity<KIND>();
+#pragma unroll
+  for (int j = 0; j < kGroupIPT; ++j) {
+    if (j >= nv) break;
+    if ((fl >> j) & 1u) tail = agg_identity<KIND>();
+    Agg<KIND> r;
+    r.cnt = 1;
+    r.sum = r.mn = r.mx = need_vals ? word[j] : 0ull;
+    tail = agg_combine<KIND>(tail, r);
+  }
+  // segmented inclusive scan over lanes: a lane with a group start restarts
+  Agg<KIND> run = tail;
+  bool seg = fl != 0u;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const Agg<KIND> up = agg_shfl_up<KIND>(run, o);
+    const bool useg = __shfl_up_sync(0xffffffffu, seg, o);
+    if (lane >= o && !seg) {
+      run = agg_combine<KIND>(up, run);
+      seg = useg;
+    }
+  }
+  // the part of the lane's first group in earlier lanes, and whether that
+  // group began inside this warp
+  Agg<KIND> cur = agg_shfl_up<KIND>(run, 1);
+  bool cur_started = __shfl_up_sync(0xffffffffu, seg, 1);
+  bool cur_rows = lane > 0;
+  if (lane == 0) {
+    cur = agg_identity<KIND>();
+    cur_started = false;
+  }
+  u32 cur_gid = gfirst - 1u;
+  // pass 2: write every group that ends inside the lane
+#pragma unroll 1
+  for (int j = 0; j < nv; ++j) {
+    if ((fl >> j) & 1u) {
+      if (cur_rows) {
+        if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
+        else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);  // the warp's first group, begun earlier
+      }
+      cur = agg_identity<KIND>();
+      cur_started = true;
+      cur_gid = gfirst + __popc(fl & ((1u << j) - 1u));
+    }
+    Agg<KIND> r;
+    r.cnt = 1;
+    r.sum = r.mn = r.mx = need_vals ? word[j] : 0ull;
+    cur = agg_combine<KIND>(cur, r);
+    cur_rows = true;
+  }
+  if (nv == 0) return;
+  // the group open at the lane end ends here if the next lane starts a group,
+  // or at the warp end when the row after the warp starts one
+  if (last_lane ? end_closes : next_flag) {
+    if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
+    else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);
+  } else if (last_lane) {
+    slot_store<KIND>(a, c, 2 * w + 1, cur_gid, cur_started ? 1u : 0u, cur);  // open past the warp end
+  }
 }
 
 template <typename K>
-__global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps) {
+__global__ void __launch_bounds__(256) k_group_reduce(GroupArgs a, u64 nwarps) {
   const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (w >= nwarps) return;
+  if (w >= nwarps) return;  // whole warps exit together
   const K* sk = (const K*)a.skeys;
   const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
-  const u32 gbase = a.warp_base[w];
-  const u32 le = (2u << lane) - 1u;
-  u32 fm[kGroupIPT], pr[kGroupIPT];
-  u32 gcount = 0;
-  K kv[kGroupIPT], kl[kGroupIPT];
+  const u64 r0 = wbeg + (u64)lane * kGroupIPT;
+  const int nv = r0 >= wend ? 0 : (int)min((u64)kGroupIPT, wend - r0);
+  K kv[kGroupIPT];
+  if (nv == kGroupIPT && (kGroupIPT * sizeof(K)) % 16 == 0) {
 #pragma unroll
-  for (int s = 0; s < kGroupIPT; ++s) {  // loads first
-    const u64 row = wbeg + (u64)s * 32 + lane;
-    const bool valid = row < wend;
-    kv[s] = valid ? sk[row] : (K)0;
-    kl[s] = (lane == 0 && valid && row > 0) ? sk[row - 1] : (K)0;
-    pr[s] = valid ? (a.values_sorted ? (u32)row : a.perm[row]) : 0u;
+    for (int q = 0; q < kGroupIPT * (int)sizeof(K) / 16; ++q)
+      reinterpret_cast<uint4*>(kv)[q] = __ldg(reinterpret_cast<const uint4*>(sk + r0) + q);
+  } else {
+#pragma unroll
+    for (int j = 0; j < kGroupIPT; ++j) kv[j] = j < nv ? sk[r0 + j] : (K)0;
   }
+  u32 pr[kGroupIPT];
+  if (!a.values_sorted) {
 #pragma unroll
-  for (int s = 0; s < kGroupIPT; ++s) {
-    const u64 row = wbeg + (u64)s * 32 + lane;
-    const bool valid = row < wend;
-    K k = kv[s], kp = 0;
-    kp = __shfl_up_sync(0xffffffffu, k, 1);
-    if (lane == 0) kp = kl[s];
-    const bool f = valid && (row == 0 || k != kp || packed_has_nan<K>(a.pack, k));
-    fm[s] = __ballot_sync(0xffffffffu, f);
-    if (f) {
-      // unique key columns of the new group
-      const u32 gid = gbase + gcount + __popc(fm[s] & le) - 1u;
-      for (int j = 0; j < a.pack.ncols; ++j) {
-        const ColDesc& c = a.pack.c[j];
-        if (!a.uniq_out[j]) continue;
-        if (dtype_is_float(c.dtype)) {
-          // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
-          const u32 krow = a.perm ? a.perm[row] : (u32)row;
-          store_raw(a.uniq_out[j], c.dtype, gid, load_raw(c.ptr, c.dtype, krow));
-        } else {
-          const u64 field = c.bits ? (((u64)k >> c.shift) & (c.bits >= 64 ? ~0ull : ((1ull << c.bits) - 1ull))) : 0ull;
-          store_raw(a.uniq_out[j], c.dtype, gid, untransform_int(c.dtype, c.flags, field + c.tmin));
-        }
+    for (int j = 0; j < kGroupIPT; ++j) pr[j] = j < nv ? a.perm[r0 + j] : 0u;
+  } else {
+#pragma unroll
+    for (int j = 0; j < kGroupIPT; ++j) pr[j] = (u32)(r0 + j);
+  }
+  // group starts: the key differs from the previous row's (a NaN key is a group of its own)
+  K prev = __shfl_up_sync(0xffffffffu, kv[kGroupIPT - 1], 1);
+  if (lane == 0) prev = wbeg > 0 ? sk[wbeg - 1] : (K)0;
+  u32 fl = 0;
+#pragma unroll
+  for (int j = 0; j < kGroupIPT; ++j) {
+    const K kp = j ? kv[j - 1] : prev;
+    const bool f = j < nv && (r0 + j == 0 || kv[j] != kp || packed_has_nan<K>(a.pack, kv[j]));
+    fl |= (u32)f << j;
+  }
+  // group id of the lane's first start: warp base + starts in earlier lanes
+  const u32 cnt = __popc(fl);
+  u32 inc = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const u32 gfirst = a.warp_base[w] + inc - cnt;
+  // unique key columns of every group starting in the lane
+  for (u32 m = fl; m; m &= m - 1) {
+    const int j = __ffs(m) - 1;
+    const u32 gid = gfirst + __popc(fl & ((1u << j) - 1u));
+    const u64 row = r0 + j;
+    for (int jc = 0; jc < a.pack.ncols; ++jc) {
+      const ColDesc& cd = a.pack.c[jc];
+      if (!a.uniq_out[jc]) continue;
+      if (dtype_is_float(cd.dtype)) {
+        // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
+        const u32 krow = a.perm ? a.perm[row] : (u32)row;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, load_raw(cd.ptr, cd.dtype, krow));
+      } else {
+        const u64 field = cd.bits ? (((u64)kv[j] >> cd.shift) & (cd.bits >= 64 ? ~0ull : ((1ull << cd.bits) - 1ull))) : 0ull;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, untransform_int(cd.dtype, cd.flags, field + cd.tmin));
       }
     }
-    gcount += __popc(fm[s]);
   }
-  bool closed_end = true;
-  if (wend < a.n) closed_end = row_flag<K>(a, sk, wend);
+  const int last = (int)((wend - 1 - wbeg) / kGroupIPT);  // lane holding the warp's last row
+  const bool end_closes = wend < a.n ? row_flag<K>(a, sk, wend) : true;
+  const bool next_flag = __shfl_down_sync(0xffffffffu, fl & 1u, 1) != 0u;
   for (int c = 0; c < a.nvals; ++c) {
     switch (a.v[c].kind) {
-      case VK_F: reduce_column<VK_F>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
-      case VK_I: reduce_column<VK_I>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
-      default: reduce_column<VK_U>(a, c, fm, pr, w, wbeg, wend, gbase, closed_end); break;
+      case VK_F: reduce_lane_column<VK_F>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      case VK_I: reduce_lane_column<VK_I>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      default: reduce_lane_column<VK_U>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
     }
   }
 }
