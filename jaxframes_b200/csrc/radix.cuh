@@ -1531,7 +1531,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
 
 template <typename K>
 inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
-  if (rq.nwords > 1 && rq.digit_mode == DIG_BITS) rq.max_digit_bits = 8;
+  // payload-carrying sorts use 8- or 9-bit digits (shared memory for the
+  // staged words leaves no room for wider histograms); 9 saves a pass for
+  // keys of 25..27 bits
+  if (rq.nwords > 1 && rq.digit_mode == DIG_BITS) rq.max_digit_bits = 9;
   int rb;
   if (rq.digit_mode == DIG_MOD) {
     rb = rq.modulus <= 256 ? 8 : rq.modulus <= 512 ? 9 : rq.modulus <= 1024 ? 10 : 11;
@@ -1540,12 +1543,15 @@ inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaSt
     int w = ceil_div(rq.total_bits, npass);
     rb = w <= 8 ? 8 : w;
   }
-  if (rq.nwords > 1) {  // payload-carrying sorts use 8-bit digits
-    if (rq.digit_mode == DIG_BITS) rq.max_digit_bits = 8;
-    switch (rq.nwords) {
-      case 2: return run_radix<K, 8, 2>(rq, n, b, err, s);
-      case 3: return run_radix<K, 8, 3>(rq, n, b, err, s);
-      case 4: return run_radix<K, 8, 4>(rq, n, b, err, s);
+  if (rq.nwords > 1) {
+    if (rb > 9) return fail(JFX_ERR_ARG, "digit width %d with payload words unsupported", rb);
+    switch (rq.nwords * 16 + rb) {
+      case 2 * 16 + 8: return run_radix<K, 8, 2>(rq, n, b, err, s);
+      case 3 * 16 + 8: return run_radix<K, 8, 3>(rq, n, b, err, s);
+      case 4 * 16 + 8: return run_radix<K, 8, 4>(rq, n, b, err, s);
+      case 2 * 16 + 9: return run_radix<K, 9, 2>(rq, n, b, err, s);
+      case 3 * 16 + 9: return run_radix<K, 9, 3>(rq, n, b, err, s);
+      case 4 * 16 + 9: return run_radix<K, 9, 4>(rq, n, b, err, s);
     }
     return fail(JFX_ERR_ARG, "1..4 payload words supported");
   }
