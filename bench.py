@@ -92,6 +92,14 @@ def c4_keys(nblocks=65_536, block=4096, seed=45):
     return out.reshape(-1)
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# k_onesweep launch of this workload, averaged over the six passes of one
+# join call, from the ncu capture summarised in
+# profiles/join_10Mx5M_launch_list.md (cold-cache replays; the writes that
+# stay in L2 between passes are not counted).
+ONESWEEP_DRAM_BYTES_PER_LAUNCH = 90.1e6
+
+
 def join_model_bytes(nl, nr, m):
     """Algorithmic bytes of the join: SORT(L) + SORT(R) + merge read + output,
     with K = 8 (int64 key), I = 4, P = ceil(23 / 11) = 3 passes."""
@@ -355,7 +363,8 @@ def run_gpu(args):
             "model_frac": model / (ms / 1000) / 1e9 / hbm,
             "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix pass)", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
-                         "traffic": None, "peak_source": peak_src,
+                         "traffic": ONESWEEP_DRAM_BYTES_PER_LAUNCH, "traffic_unit": "bytes per launch (ncu)",
+                         "algorithmic_bytes_per_launch": pass_bytes, "peak_source": peak_src,
                          "launches": int(pl.value), "avg_launch_ms": pass_ms},
             "e2e": {"value": (NL + NR) * world / (e2e_ms / 1000), "unit": "rows/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},

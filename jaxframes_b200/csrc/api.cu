@@ -153,10 +153,13 @@ struct JoinBuffers {
   u64 *off, *partial, *total, *win, *stats;
   u32* cw[2][kMaxWords];  // carried payload words of each side, sorted order
 };
-static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, JoinBuffers& j) {
+// b: the left side's sort buffers, br the right side's (the two sorts run
+// on two streams at once).
+static void carve_join(Arena& ar, u64 nl, u64 nr, Common& c, SortBuffers& b, SortBuffers& br, JoinBuffers& j) {
   take_common(ar, c);
   u64 nmax = std::max(nl, nr);
-  take_sort_buffers(ar, nmax, b, kMaxWords);
+  take_sort_buffers(ar, nl, b, kMaxWords);
+  take_sort_buffers(ar, nr, br, kMaxWords);
   j.skL = ar.take<u64>(nl ? nl : 1);
   j.skR = ar.take<u64>(nr ? nr : 1);
   j.pL = ar.take<u32>(nl ? nl : 1);
@@ -200,6 +203,7 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
 
 // ---------------------------------------------------------------- learned ---
 struct LearnedBuffers {
+  u32* pos;   // predicted position of each key, in row order
   u32* spos;  // predicted position of each key, in sorted order
   u64* sample;
   u64* ssorted;
@@ -217,6 +221,7 @@ struct LearnedBuffers {
 static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBuffers& l) {
   take_common(ar, c);
   take_sort_buffers(ar, n, b, 3);
+  l.pos = ar.take<u32>(n ? n : 1);
   l.spos = ar.take<u32>(n ? n : 1);
   l.s = n / kSampleStride;
   l.sample = ar.take<u64>(l.s + 1);
@@ -331,6 +336,27 @@ static int check_n(int64_t n) {
 }
 
 
+// A second stream (and two events) per host thread and device, created on
+// first use, so that independent sorts of one call can overlap.
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+static int side_stream(SideStream** out) {
+  thread_local SideStream per_dev[128];
+  int dev = -1;
+  JFX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(JFX_ERR_ARG, "device ordinal %d out of range", dev);
+  SideStream& ss = per_dev[dev];
+  if (!ss.stream) {
+    JFX_CUDA(cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking));
+    JFX_CUDA(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+    JFX_CUDA(cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming));
+  }
+  *out = &ss;
+  return JFX_OK;
+}
+
 // ------------------------------------------------ sort without allocation ---
 // Scratch of jfx_sort_static: a fixed device array in this library instead of
 // a caller workspace.  Every device that loads the library holds it until the
@@ -441,7 +467,8 @@ size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2) {
     }
     case JFX_WS_JOIN: {
       JoinBuffers j;
-      carve_join(ar, a, bn, c, b, j);
+      SortBuffers br;
+      carve_join(ar, a, bn, c, b, br, j);
       break;
     }
     case JFX_WS_PARTITION:
@@ -810,9 +837,9 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
   cudaStream_t s = as_stream(stream);
   Arena ar(workspace, workspace_bytes);
   Common c;
-  SortBuffers b;
+  SortBuffers b, br;
   JoinBuffers j;
-  carve_join(ar, (u64)nl, (u64)nr, c, b, j);
+  carve_join(ar, (u64)nl, (u64)nr, c, b, br, j);
   if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   // a single key is sorted by ParallelRadixSort (narrow ints keep the
@@ -871,9 +898,19 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
     }
     carried[side] = words;
   }
+  // the right side sorts on a second stream while the left side sorts on s
+  cudaStream_t s2 = s;
+  SideStream* ss = nullptr;
+  if (nl && nr) {
+    JFX_TRY(side_stream(&ss));
+    s2 = ss->stream;
+    JFX_CUDA(cudaEventRecord(ss->fork, s));
+    JFX_CUDA(cudaStreamWaitEvent(s2, ss->fork, 0));
+  }
   for (int side = 0; side < 2; ++side) {
     const u64 ns = side ? (u64)nr : (u64)nl;
     if (!ns) continue;
+    const cudaStream_t st = side ? s2 : s;
     RadixRequest rq;
     rq.pack = side ? pr : pl;
     rq.total_bits = total_bits;
@@ -889,7 +926,11 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
     } else {
       rq.perm_out = side ? j.pR : j.pL;
     }
-    JFX_TRY(radix_sort(rq, ns, b, c.err, s));
+    JFX_TRY(radix_sort(rq, ns, side ? br : b, c.err, st));
+  }
+  if (ss) {
+    JFX_CUDA(cudaEventRecord(ss->join, s2));
+    JFX_CUDA(cudaStreamWaitEvent(s, ss->join, 0));
   }
   // forward counts drive inner/left joins, swapped counts right joins; the
   // unmatched rows of a side need that side's counts
@@ -1290,14 +1331,20 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   // model once per key and sorts by the position, carrying the key (two
   // words) and the row id; the last pass writes the key as one u64
   {
-    jfx_column col{keys, JFX_U64, 0u};
+    // positions once (row order), then a plain sort of that uint32 column:
+    // its histogram kernel counts the first pass's tiles, so every pass runs
+    // in two phases with the lean integer-key first pass
+    k_model_positions<<<grid_for(N, 256), 256, 0, s>>>(keys, N, l.model, l.pos), note_launch();
+    JFX_CUDA(cudaGetLastError());
+    jfx_column col{l.pos, JFX_U32, 0u};
     RadixRequest rq;
     JFX_TRY(build_pack(&col, 1, 0u, false, rq.pack));
-    rq.pack.c[0].bits = 64;
-    rq.key_mode = KEY_MODEL;
-    rq.digit_mode = DIG_BITS;
-    rq.model = l.model;
     rq.total_bits = std::max(1, bit_length(npos - 1));
+    rq.pack.c[0].tmin = 0;
+    rq.pack.c[0].bits = rq.total_bits;
+    rq.pack.c[0].shift = 0;
+    rq.key_mode = KEY_PACK;
+    rq.digit_mode = DIG_BITS;
     rq.key64 = false;
     rq.nwords = 3;
     rq.pfirst[0] = PayloadSrc{(const unsigned char*)keys, 8u, 0u};

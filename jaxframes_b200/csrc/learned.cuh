@@ -163,6 +163,21 @@ __global__ void __launch_bounds__(1024) k_leaf_finalize(const u64* sx, u64 s, u6
   }
 }
 
+// Predicted position of every key, in row order.
+__global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n, const ModelRef* mp, u32* pos) {
+  const ModelRef m = *mp;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  constexpr int U = 4;
+  for (u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * U) {
+    u64 k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) k[u] = i0 + u * stride < n ? __ldg(keys + i0 + u * stride) : 0ull;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (i0 + u * stride < n) pos[i0 + u * stride] = model_pos(m, k[u]);
+  }
+}
+
 // ------------------------------------------------------------------ fix-up ---
 constexpr int kFindTile = 2048, kFindThreads = 256;
 constexpr int kFixMaxRun = 6144;   // longest run the shared-memory block sort takes

@@ -1531,10 +1531,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
 
 template <typename K>
 inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStream_t s) {
-  // payload-carrying sorts use 8- or 9-bit digits (shared memory for the
-  // staged words leaves no room for wider histograms); 9 saves a pass for
-  // keys of 25..27 bits
-  if (rq.nwords > 1 && rq.digit_mode == DIG_BITS) rq.max_digit_bits = 9;
+  // payload-carrying sorts use 8- to 10-bit digits (shared memory for the
+  // staged words leaves no room for wider histograms); 9 and 10 save a pass
+  // for keys of 25..30 bits
+  if (rq.nwords > 1 && rq.digit_mode == DIG_BITS) rq.max_digit_bits = 10;
   int rb;
   if (rq.digit_mode == DIG_MOD) {
     rb = rq.modulus <= 256 ? 8 : rq.modulus <= 512 ? 9 : rq.modulus <= 1024 ? 10 : 11;
@@ -1544,7 +1544,7 @@ inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaSt
     rb = w <= 8 ? 8 : w;
   }
   if (rq.nwords > 1) {
-    if (rb > 9) return fail(JFX_ERR_ARG, "digit width %d with payload words unsupported", rb);
+    if (rb > 10) return fail(JFX_ERR_ARG, "digit width %d with payload words unsupported", rb);
     switch (rq.nwords * 16 + rb) {
       case 2 * 16 + 8: return run_radix<K, 8, 2>(rq, n, b, err, s);
       case 3 * 16 + 8: return run_radix<K, 8, 3>(rq, n, b, err, s);
@@ -1552,6 +1552,9 @@ inline int run_radix_k(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaSt
       case 2 * 16 + 9: return run_radix<K, 9, 2>(rq, n, b, err, s);
       case 3 * 16 + 9: return run_radix<K, 9, 3>(rq, n, b, err, s);
       case 4 * 16 + 9: return run_radix<K, 9, 4>(rq, n, b, err, s);
+      case 2 * 16 + 10: return run_radix<K, 10, 2>(rq, n, b, err, s);
+      case 3 * 16 + 10: return run_radix<K, 10, 3>(rq, n, b, err, s);
+      case 4 * 16 + 10: return run_radix<K, 10, 4>(rq, n, b, err, s);
     }
     return fail(JFX_ERR_ARG, "1..4 payload words supported");
   }
