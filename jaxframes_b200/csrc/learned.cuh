@@ -226,6 +226,19 @@ __device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
 
 // Lists the runs of equal predicted position that start in this CTA's tile
 // and contain an inversion.
+// First set bit of the bitmap w in [lo, hi), or hi: a word at a time.
+__device__ __forceinline__ u32 first_bit_in(const u32* w, u32 lo, u32 hi) {
+  for (u32 q = lo; q < hi;) {
+    const u32 bits = w[q >> 5] >> (q & 31);
+    if (bits) {
+      const u32 r = q + __ffs(bits) - 1;
+      return r < hi ? r : hi;
+    }
+    q = (q | 31) + 1;
+  }
+  return hi;
+}
+
 __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals, const u32* spos, u64 n,
                                                            FixLists L) {
   __shared__ u64 sk[kFindTile + 1];
@@ -276,9 +289,8 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
         lastp = (w << 5) + 31 - __clz(b);
       }
     }
-    u32 cinv = 0xffffffffu;
-    for (u32 q = off; q < first && cinv == 0xffffffffu; ++q)
-      if ((ib[q >> 5] >> (q & 31)) & 1u) cinv = q;
+    const u32 cq = first_bit_in(ib, off, first);
+    const u32 cinv = cq < first ? cq : 0xffffffffu;
     L.last_start[blockIdx.x] = lastp == 0xffffffffu ? lastp : (u32)(base + lastp);
     L.carried_inv[blockIdx.x] = cinv == 0xffffffffu ? cinv : (u32)(base + cinv);
   }
@@ -302,9 +314,7 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
       s_open = (int)i;
       continue;
     }
-    bool inv = false;
-    for (u32 q = i + 1; q < e && !inv; ++q) inv = (ib[q >> 5] >> (q & 31)) & 1u;
-    if (!inv) continue;
+    if (first_bit_in(ib, i + 1, e) >= e) continue;  // no inversion in the run
     if (e - i > (u32)kFixSmall) {
       fix_record(L, base + i, base + e);
       continue;
@@ -338,11 +348,9 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
   const u32 i = (u32)s_open;
   const u32 p0 = sp[i];
   const u64 k0 = sk[i];
-  bool inv = false, distinct = false;
-  for (u32 q = i + 1; q < len; ++q) {
-    inv |= (ib[q >> 5] >> (q & 31)) & 1u;
-    distinct |= sk[q] != k0;
-  }
+  bool inv = first_bit_in(ib, i + 1, len) < len, distinct = false;
+  for (u32 q = i + 1 + lane; q < len; q += 32) distinct |= sk[q] != k0;
+  distinct = __any_sync(0xffffffffu, distinct);
   u64 prev_key = sk[len - 1];
   u64 pos = t1;
   u64 e = n;
