@@ -805,7 +805,7 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   if (rq.key64) k_group_reduce<u64><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
   else k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
   JFX_CUDA(cudaGetLastError());
-  k_group_fixup<<<(unsigned)((ga.nslots + 255) / 256), 256, 0, s>>>(ga), note_launch();
+  k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
   JFX_CUDA(cudaGetLastError());
   u64* host = g_host.get();
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
@@ -1563,7 +1563,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
     JFX_TRY(device_exclusive_scan<u32>(bb.g.warp_count, bb.g.nwarps, bb.g.warp_base, bb.g.total, bb.g.partial, s));
     JFX_CUDA(cudaMemsetAsync(bb.g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
     k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, bb.g.nwarps), note_launch();
-    k_group_fixup<<<(unsigned)((ga.nslots + 255) / 256), 256, 0, s>>>(ga), note_launch();
+    k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
   } else {
     JFX_CUDA(cudaMemsetAsync(bb.g.total, 0, sizeof(u32), s));
   }

@@ -528,30 +528,57 @@ __device__ __forceinline__ Agg<KIND> slot_load(const GroupArgs& a, int c, u64 i)
   return s;
 }
 
+// The records [i, end) of group g (empty records skipped), combined in row
+// order by one warp: lane l folds a contiguous share of the records, then a
+// tree in lane order joins the shares, so a group spanning many warps costs
+// its record count / 32 steps, not one step per record.
 template <int KIND>
-__device__ void fixup_column(const GroupArgs& a, int c, u64 i, u32 g) {
-  Agg<KIND> s = slot_load<KIND>(a, c, i);
-  for (u64 j = i + 1; j < a.nslots; ++j) {
-    const u32 gj = a.slot_gid[j];
-    if (gj == kEmptySlot) continue;
-    if (gj != g || a.slot_started[j]) break;
-    s = agg_combine<KIND>(s, slot_load<KIND>(a, c, j));
+__device__ void fixup_column(const GroupArgs& a, int c, u64 i, u64 end, u32 g, int lane) {
+  const u64 cnt = end - i, share = (cnt + 31) / 32;
+  const u64 j0 = i + (u64)lane * share, j1 = min(end, j0 + share);
+  Agg<KIND> s = agg_identity<KIND>();
+  for (u64 j = j0; j < j1; ++j)
+    if (a.slot_gid[j] == g) s = agg_combine<KIND>(s, slot_load<KIND>(a, c, j));
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    Agg<KIND> up;
+    up.sum = __shfl_down_sync(0xffffffffu, s.sum, o);
+    up.mn = __shfl_down_sync(0xffffffffu, s.mn, o);
+    up.mx = __shfl_down_sync(0xffffffffu, s.mx, o);
+    up.cnt = __shfl_down_sync(0xffffffffu, s.cnt, o);
+    if ((lane & (2 * o - 1)) == 0 && lane + o < 32) s = agg_combine<KIND>(s, up);
   }
-  agg_finalize<KIND>(a.v[c], g, s);
+  if (lane == 0) agg_finalize<KIND>(a.v[c], g, s);
 }
 
-// One thread per partial record; the record holding the group's first row
-// combines the group's records in row order and writes the result.
+// One warp per partial record; the warp of the record holding the group's
+// first row finds the group's following records (same group id, not a group
+// start; empty records in between) 32 at a time and combines them.
 __global__ void __launch_bounds__(256) k_group_fixup(GroupArgs a) {
-  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nslots) return;
+  const u64 i = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= a.nslots) return;  // whole warps
   const u32 g = a.slot_gid[i];
   if (g == kEmptySlot || !a.slot_started[i]) return;
+  u64 end = a.nslots;
+  for (u64 b = i + 1; b < a.nslots; b += 32) {
+    const u64 j = b + lane;
+    bool stop = j >= a.nslots;
+    if (!stop) {
+      const u32 gj = a.slot_gid[j];
+      stop = gj != kEmptySlot && (gj != g || a.slot_started[j]);
+    }
+    const u32 sm = __ballot_sync(0xffffffffu, stop);
+    if (sm) {
+      end = b + __ffs(sm) - 1;
+      break;
+    }
+  }
   for (int c = 0; c < a.nvals; ++c) {
     switch (a.v[c].kind) {
-      case VK_F: fixup_column<VK_F>(a, c, i, g); break;
-      case VK_I: fixup_column<VK_I>(a, c, i, g); break;
-      default: fixup_column<VK_U>(a, c, i, g); break;
+      case VK_F: fixup_column<VK_F>(a, c, i, end, g, lane); break;
+      case VK_I: fixup_column<VK_I>(a, c, i, end, g, lane); break;
+      default: fixup_column<VK_U>(a, c, i, end, g, lane); break;
     }
   }
 }
