@@ -443,7 +443,7 @@ __device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u6
 }
 
 template <typename K>
-__global__ void __launch_bounds__(256) k_group_reduce(GroupArgs a, u64 nwarps) {
+__global__ void __launch_bounds__(256, 4) k_group_reduce(GroupArgs a, u64 nwarps) {  // 4 CTAs per SM
   const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nwarps) return;  // whole warps exit together
