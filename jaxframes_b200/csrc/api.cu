@@ -1495,7 +1495,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   a.status_next = bb.status[1];
   a.tile_counter = bb.counters;
   a.seg.pass_index = 0;
-  JFX_TRY((launch_pass<u32, RB, 2>(a, (u64)n, s, bb.max_tiles)));
+  JFX_TRY((launch_pass<u32, RB, 1>(a, (u64)n, s, bb.max_tiles)));  // one plain int32 key column
   {
     const u64 tot = (u64)nq * (num_partitions + 1);
     k_part_offsets<<<grid_for(tot, 256), 256, 0, s>>>(bb.row_base, bb.base, (u32)nq, npass, RADIX,

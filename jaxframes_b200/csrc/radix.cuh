@@ -474,9 +474,16 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
         if (b1) key[i] |= (K)((((u64)r1[i] ^ flip1) - tmin1) << sh1);
       }
     }
+    if (a.digit_mode == DIG_BITS) {
 #pragma unroll
-    for (int i = 0; i < IPT; ++i)
-      rd[i] = (full || toff + i * 32 < tile_n) ? (u32)(key[i] >> a.shift) & mask : (u32)RADIX;
+      for (int i = 0; i < IPT; ++i)
+        rd[i] = (full || toff + i * 32 < tile_n) ? (u32)(key[i] >> a.shift) & mask : (u32)RADIX;
+    } else {  // the batched partition pass: hash digit
+#pragma unroll
+      for (int i = 0; i < IPT; ++i)
+        rd[i] = (full || toff + i * 32 < tile_n) ? digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model)
+                                                 : (u32)RADIX;
+    }
   } else if (two_first) {
     // two key columns: both columns' loads for 8 items, then pack
 #pragma unroll
@@ -662,6 +669,53 @@ __global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) 
           continue;
         }
         kout[g] = kk[i];
+        if (NW >= 2 && a.vout64) {
+          a.vout64[g] = (unsigned long long)spay[uu[i]] | ((unsigned long long)spay[TILE + uu[i]] << 32);
+#pragma unroll
+          for (int w = 2; w < NW; ++w) a.vout[w][g] = spay[w * TILE + uu[i]];
+        } else {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + uu[i]];
+        }
+      }
+    }
+    if (a.status_next)
+      for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
+    return;
+  }
+  if (full) {
+    // full tile, other output forms (original-dtype keys, descending
+    // positions, query-tagged keys): the same unrolled slots
+    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+    const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
+#pragma unroll
+    for (int i0 = 0; i0 < IPT; i0 += 8) {
+      K kk[8];
+      u32 gg[8], uu[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const u32 j = (i0 + i) * THREADS + tid;
+        kk[i] = skeys[j];
+        uu[i] = sidx[j];
+        gg[i] = sbase[sdig[j]] + j;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (gg[i] - row0 >= span) {
+          atomicOr(a.err, DERR_BOUNDS);
+          continue;
+        }
+        const u64 g = a.reverse ? a.n - 1 - (u64)gg[i] : (u64)gg[i];
+        if (rsz) {
+          const u64 v = untransform_int(a.raw_dtype, a.raw_flags, (u64)kk[i] + a.raw_tmin);
+          if (rsz == 4) ((u32*)a.raw_out)[g] = (u32)v;
+          else if (rsz == 8) ((u64*)a.raw_out)[g] = v;
+          else store_raw(a.raw_out, a.raw_dtype, g, v);
+        } else if (a.segmented && a.seg.key_shift_q) {
+          kout[g] = (kk[i] & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
+        } else {
+          kout[g] = kk[i];
+        }
         if (NW >= 2 && a.vout64) {
           a.vout64[g] = (unsigned long long)spay[uu[i]] | ((unsigned long long)spay[TILE + uu[i]] << 32);
 #pragma unroll
