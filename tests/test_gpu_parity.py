@@ -1,7 +1,7 @@
 """GPU parity: the product API (through libjfx.so) against the oracle and the
 reference tests' known answers.  Bit-exact for orders, keys, counts, min/max,
 index pairs and partition assignments; float sums within 2^-16 * sum(|x|)
-per group (the tolerance of the north-star contract)."""
+per group (the tolerance stated for float32 sums and means)."""
 
 import numpy as np
 import pytest
