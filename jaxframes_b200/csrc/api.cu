@@ -291,7 +291,6 @@ struct BatchBuffers {
   GroupBuffers g;
   u64 max_tiles;
 };
-constexpr int kBatchRB = 10;  // digit width of the batched passes (RADIX 1024)
 
 static void carve_batch(Arena& ar, u64 n, u64 nq, Common& c, BatchBuffers& b) {
   take_common(ar, c);

@@ -17,9 +17,8 @@
 
 namespace jfx {
 
-constexpr int kBatchTile = PassLayout<u32, 8>::TILE;  // every pass config uses this tile
-static_assert(PassLayout<u32, 10>::TILE == kBatchTile && PassLayout<u32, 11>::TILE == kBatchTile,
-              "batched passes share one tile size");
+constexpr int kBatchRB = 10;  // digit width of the batched passes (RADIX 1024)
+constexpr int kBatchTile = PassLayout<u32, kBatchRB>::TILE;  // rows per tile of every batched pass
 
 __global__ void k_seg_setup(const int64_t* qoff, u32 nq, u64* row_base, u32* tile_cnt, u32* err) {
   for (u32 q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) {

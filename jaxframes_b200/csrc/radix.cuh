@@ -26,17 +26,21 @@ namespace jfx {
 // look-back status word: [31:30] flag, [29:0] count
 constexpr u32 ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_ERR = 3u << 30, ST_CNT = (1u << 30) - 1;
 
-template <int RB>
+// 256 threads per tile.  Items per thread: 8 (2048-row tiles) for the
+// common 8/9-bit digits with one payload word -- fewer registers, more CTAs
+// per SM -- and 16 otherwise, where the digit histograms and staged words
+// make a bigger tile pay.
+template <int RB, int NW = 1>
 struct RadixCfg {
   static constexpr int THREADS = 256;
-  static constexpr int IPT = 16;
+  static constexpr int IPT = (NW == 1 && RB <= 9) ? 8 : 16;
 };
 
 constexpr int kMaxWords = 4;  // payload words a pass can carry per row
 
 template <typename K, int RB, int NW = 1>
 struct PassLayout {
-  static constexpr int THREADS = RadixCfg<RB>::THREADS, IPT = RadixCfg<RB>::IPT;
+  static constexpr int THREADS = RadixCfg<RB, NW>::THREADS, IPT = RadixCfg<RB, NW>::IPT;
   static constexpr int RADIX = 1 << RB, WARPS = THREADS / 32, TILE = THREADS * IPT;
   static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 4;
   static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
@@ -345,7 +349,7 @@ __device__ __forceinline__ K pack2(const PackDesc& pd, u64 r0, u64 r1) {
 // instantiation: fewer registers, more CTAs per SM); 2 = any other first pass
 // (packed or hashed columns, gathered rows, the learned position).
 template <typename K, int RB, int FM, int NW>
-__global__ void __launch_bounds__(RadixCfg<RB>::THREADS) k_onesweep(PassArgs a) {
+__global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs a) {
   constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
   constexpr int THREADS = L::THREADS, IPT = L::IPT, RADIX = L::RADIX, WARPS = L::WARPS,
@@ -871,6 +875,7 @@ struct HistIntArgs {
   // [RADIX][tiles], so that pass can run in two phases as well
   u32* tile_counts;
   u64 tiles;
+  u32 tile_rows;  // rows per tile of that pass
 };
 
 template <typename K, typename T, int RB>
@@ -883,30 +888,33 @@ __global__ void __launch_bounds__(256) k_hist_int(HistIntArgs a) {
   if (a.tile_counts) {
     // tile by tile (the radix pass's tiles): all passes' counts plus the
     // first pass's counts of this tile
-    constexpr int TILE = PassLayout<K, RB>::TILE, IPT = TILE / 256;
+    constexpr int CH = 8;  // rows per thread per chunk; a tile is 1 or 2 chunks
+    const u32 TILE = a.tile_rows;
     u32* tsh = sh + total;
     for (int i = threadIdx.x; i < total + RADIX; i += blockDim.x) sh[i] = 0u;
     __syncthreads();
     for (u64 t = blockIdx.x; t < a.tiles; t += gridDim.x) {
       const u64 base = t * TILE;
       const u32 tn = (u32)min((u64)TILE, a.n - base);
-      T raw[IPT], raw2[IPT];
+      for (u32 c0 = 0; c0 < tn; c0 += 256 * CH) {
+        T raw[CH], raw2[CH];
 #pragma unroll
-      for (int i = 0; i < IPT; ++i) {
-        const u32 r = i * 256 + threadIdx.x;
-        raw[i] = r < tn ? __ldg(col + base + r) : (T)0;
-        raw2[i] = (col2 && r < tn) ? __ldg(col2 + base + r) : (T)0;
-      }
+        for (int i = 0; i < CH; ++i) {
+          const u32 r = c0 + i * 256 + threadIdx.x;
+          raw[i] = r < tn ? __ldg(col + base + r) : (T)0;
+          raw2[i] = (col2 && r < tn) ? __ldg(col2 + base + r) : (T)0;
+        }
 #pragma unroll
-      for (int i = 0; i < IPT; ++i) {
-        if (i * 256 + threadIdx.x >= tn) break;
-        K k = (K)((((u64)raw[i] ^ a.flip) - a.tmin) << a.kshift);
-        if (col2) k |= (K)((((u64)raw2[i] ^ a.flip2) - a.tmin2) << a.kshift2);
-        atomicAdd(&tsh[(u32)(k >> a.shift[0]) & a.mask[0]], 1u);
+        for (int i = 0; i < CH; ++i) {
+          if (c0 + i * 256 + threadIdx.x >= tn) break;
+          K k = (K)((((u64)raw[i] ^ a.flip) - a.tmin) << a.kshift);
+          if (col2) k |= (K)((((u64)raw2[i] ^ a.flip2) - a.tmin2) << a.kshift2);
+          atomicAdd(&tsh[(u32)(k >> a.shift[0]) & a.mask[0]], 1u);
 #pragma unroll
-        for (int p = 0; p < 8; ++p) {
-          if (p >= a.npass) break;
-          atomicAdd(&sh[p * RADIX + ((u32)(k >> a.shift[p]) & a.mask[p])], 1u);
+          for (int p = 0; p < 8; ++p) {
+            if (p >= a.npass) break;
+            atomicAdd(&sh[p * RADIX + ((u32)(k >> a.shift[p]) & a.mask[p])], 1u);
+          }
         }
       }
       __syncthreads();
@@ -971,10 +979,10 @@ __global__ void __launch_bounds__(1024) k_hist_scan(const u32* hist, u32* base) 
 
 // counts[d][tile] (digit-major, so the scan reads rows) of digit
 // (key >> shift) & mask; one CTA per tile.
-template <typename K, int RB>
+template <typename K, int RB, int NW>
 __global__ void __launch_bounds__(256) k_tile_count(const K* keys, u64 n, int shift, u32 mask, u32* counts,
                                                     u64 tiles) {
-  constexpr int RADIX = 1 << RB, TILE = PassLayout<K, RB>::TILE, IPT = TILE / 256;
+  constexpr int RADIX = 1 << RB, TILE = PassLayout<K, RB, NW>::TILE, IPT = TILE / 256;
   constexpr int NH = RB <= 9 ? 8 : RB == 10 ? 4 : 2;  // histogram copies (fewer same-address atomics)
   __shared__ u32 h[NH][RADIX];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1426,7 +1434,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   rq.npass = npass;
   JFX_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)npass * RADIX * sizeof(u32), s));
   JFX_CUDA(cudaMemsetAsync(b.counters, 0, 64 * sizeof(u32), s));
-  const u64 tiles = (u64)ceil_div(n, PassLayout<K, RB>::TILE);
+  const u64 tiles = (u64)ceil_div(n, PassLayout<K, RB, NW>::TILE);
   JFX_CUDA(cudaMemsetAsync(b.status[0], 0, tiles * RADIX * sizeof(u32), s));
 
   // the passes after the first of a plain digit sort run in two phases (no
@@ -1496,6 +1504,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       if (first_two_phase) {
         hi.tile_counts = b.status[1];
         hi.tiles = tiles;
+        hi.tile_rows = (u32)PassLayout<K, RB, NW>::TILE;
         g = (int)std::min<u64>(tiles, (u64)device_sm_count() * 8);
         sm += (size_t)RADIX * sizeof(u32);
       }
@@ -1556,7 +1565,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       // status[1] holds this pass's tile counts, status[0] its tile bases
       // (pass 0, the only look-back pass, is done with both by now)
       const u32 mask_p = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
-      k_tile_count<K, RB><<<(unsigned)tiles, 256, 0, s>>>((const K*)a.keys_in, n, shift[p], mask_p, b.status[1],
+      k_tile_count<K, RB, NW><<<(unsigned)tiles, 256, 0, s>>>((const K*)a.keys_in, n, shift[p], mask_p, b.status[1],
                                                            tiles), note_launch();
       k_tile_scan<RB><<<RADIX, 256, 0, s>>>(b.status[1], tiles, a.bin_base, b.status[0]), note_launch();
       JFX_CUDA(cudaGetLastError());
