@@ -1012,25 +1012,43 @@ __global__ void __launch_bounds__(256) k_tile_count(const K* keys, u64 n, int sh
 }
 
 // base[d][t] = bin_base[d] + sum over t' < t of counts[d][t'] (mod 2^32:
-// rows < 2^30).  One CTA per digit row, 4096 tiles per round.
-template <int RB>
-__global__ void __launch_bounds__(256) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base) {
-  constexpr int PER = 16;
-  __shared__ u32 wsum[8];
+// rows < 2^30).  One CTA of T threads per digit row, 16 T tiles per round:
+// coalesced loads into shared memory (padded one word in 32, so a thread's
+// 16 consecutive entries sit in distinct banks across the warp), a block scan
+// of the thread sums, and coalesced stores of the bases.  T = 1024 for long
+// rows; T = 256 for short ones, where the small CTAs leave room for the other
+// kernels in flight (the two sides of a join sort concurrently).
+constexpr int kTileScanPer = 16;
+template <int T>
+constexpr size_t tile_scan_smem() { return (size_t)(T * kTileScanPer + T * kTileScanPer / 32) * sizeof(u32); }
+__device__ __forceinline__ u32 tile_scan_slot(u32 i) { return i + (i >> 5); }
+
+template <int T>
+__global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base) {
+  constexpr int PER = kTileScanPer, CH = T * PER;
+  static_assert(T % 32 == 0 && T <= 1024, "warps of a block");
+  extern __shared__ u32 buf[];  // [CH + CH / 32]
+  __shared__ u32 wsum[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const u32* row = counts + (u64)blockIdx.x * tiles;
   u32* out = base + (u64)blockIdx.x * tiles;
   u32 carry = bin_base[blockIdx.x];
-  for (u64 c0 = 0; c0 < tiles; c0 += 256 * PER) {
-    const u64 t0 = c0 + (u64)tid * PER;
+  for (u64 c0 = 0; c0 < tiles; c0 += CH) {
+    const u32 m = (u32)min((u64)CH, tiles - c0);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const u32 i = k * T + tid;
+      buf[tile_scan_slot(i)] = i < m ? row[c0 + i] : 0u;
+    }
+    __syncthreads();
     u32 v[PER];
     u32 sum = 0;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-      v[k] = t0 + k < tiles ? row[t0 + k] : 0u;
+      v[k] = buf[tile_scan_slot(tid * PER + k)];
       sum += v[k];
     }
-    u32 x = sum;  // inclusive scan of the thread sums: warp, then block
+    u32 x = sum;  // inclusive scan of the thread sums: warp, then across warps
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const u32 y = __shfl_up_sync(0xffffffffu, x, o);
@@ -1038,20 +1056,34 @@ __global__ void __launch_bounds__(256) k_tile_scan(const u32* counts, u64 tiles,
     }
     if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    u32 wpre = 0, total = 0;
+    if (warp == 0) {
+      const u32 w = lane < T / 32 ? wsum[lane] : 0u;
+      u32 z = w;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
-      wpre += w < warp ? wsum[w] : 0u;
-      total += wsum[w];
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      if (lane < T / 32) wsum[lane] = z - w;  // exclusive prefix of each warp
     }
-    u32 run = carry + wpre + x - sum;
+    __syncthreads();
+    u32 run = carry + wsum[warp] + x - sum;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-      if (t0 + k < tiles) out[t0 + k] = run;
+      buf[tile_scan_slot(tid * PER + k)] = run;
       run += v[k];
     }
-    carry += total;
-    __syncthreads();  // wsum is rewritten next round
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const u32 i = k * T + tid;
+      if (i < m) out[c0 + i] = buf[tile_scan_slot(i)];
+    }
+    // the last thread's running value is carry + the round's total
+    if (tid == T - 1) wsum[0] = run;
+    __syncthreads();
+    carry = wsum[0];
+    __syncthreads();  // wsum and buf are rewritten next round
   }
 }
 
@@ -1340,6 +1372,15 @@ inline u64 max_status_words(u64 n) {
   return std::max(std::max(w8, w9), std::max(w10, w11));
 }
 
+inline int launch_tile_scan(int radix, const u32* counts, u64 tiles, const u32* bin_base, u32* base, cudaStream_t s) {
+  if (tiles >= 32768)
+    k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base), note_launch();
+  else
+    k_tile_scan<256><<<radix, 256, tile_scan_smem<256>(), s>>>(counts, tiles, bin_base, base), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
+}
+
 inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b, int words = 1) {
   b.keys[0] = ar.take<u64>(n ? n : 1);
   b.keys[1] = ar.take<u64>(n ? n : 1);
@@ -1477,6 +1518,8 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       JFX_CUDA(cudaFuncSetAttribute(k_hist<K, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
       JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u64, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
       JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u32, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
+      JFX_CUDA(cudaFuncSetAttribute(k_tile_scan<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)tile_scan_smem<1024>()));
       attr = true;
     }
     if (int_key) {
@@ -1521,7 +1564,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   JFX_CUDA(cudaGetLastError());
 
   if (first_two_phase) {
-    k_tile_scan<RB><<<RADIX, 256, 0, s>>>(b.status[1], tiles, b.base, b.status[0]), note_launch();
+    JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, b.base, b.status[0], s));
     JFX_CUDA(cudaGetLastError());
   }
   u32* out_vals[kMaxWords];
@@ -1567,7 +1610,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       const u32 mask_p = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
       k_tile_count<K, RB, NW><<<(unsigned)tiles, 256, 0, s>>>((const K*)a.keys_in, n, shift[p], mask_p, b.status[1],
                                                            tiles), note_launch();
-      k_tile_scan<RB><<<RADIX, 256, 0, s>>>(b.status[1], tiles, a.bin_base, b.status[0]), note_launch();
+      JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, a.bin_base, b.status[0], s));
       JFX_CUDA(cudaGetLastError());
       a.tile_base = b.status[0];
       a.ntiles = tiles;
