@@ -348,7 +348,9 @@ __device__ __forceinline__ K pack2(const PackDesc& pd, u64 r0, u64 r1) {
 // 1 = the first pass over one plain 32/64-bit integer key column (a lean
 // instantiation: fewer registers, more CTAs per SM); 2 = any other first pass
 // (packed or hashed columns, gathered rows, the learned position).
-template <typename K, int RB, int FM, int NW>
+// TP: a two-phase pass over plain bit digits (PassArgs::tile_base set,
+// DIG_BITS, not segmented); otherwise the tile bases come from the look-back.
+template <typename K, int RB, int FM, int NW, bool TP>
 __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs a) {
   constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
@@ -560,6 +562,146 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
       const u32 off = warp * 32 * IPT + i * 32 + lane;
       rd[i] = off < tile_n ? digit_of<K>(key[i], a.digit_mode, a.shift, mask, a.modulus, model) : (u32)RADIX;
     }
+  }
+
+  if constexpr (TP) {
+    // Two-phase pass over plain bit digits: the tile's global bases are
+    // known, nothing is published, so the digit counts come out of the
+    // ranking itself (warp-private counters from zero, then per-warp
+    // prefixes), and the scatter recomputes each key's digit from the key and
+    // reads the payload already moved to sorted order: no per-row count
+    // atomics, digit or row-slot arrays in shared memory.
+    u32* wh = whist + warp * RADIX;
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 d = rd[i];
+      const bool valid = d < (u32)RADIX;
+      u32 peers = __ballot_sync(0xffffffffu, valid);
+      if (!valid) peers = ~peers;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) {
+        const u32 bit = (d >> b) & 1u;
+        const u32 bb = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bb : ~bb;
+      }
+      const int leader = 31 - __clz(peers);
+      u32 prior = 0;
+      if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
+      prior = __shfl_sync(0xffffffffu, prior, leader);
+      // bit 31 item present, bits [13, 24) digit, [0, 13) rank in the warp
+      rd[i] = valid ? 0x80000000u | (d << 13) | (prior + __popc(peers & lt)) : 0u;
+    }
+    __syncthreads();
+    for (int d = tid; d < RADIX; d += THREADS) {
+      u32 run = 0;
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) {
+        const u32 c = whist[w * RADIX + d];
+        whist[w * RADIX + d] = run;
+        run += c;
+      }
+      sexcl[d] = run;
+    }
+    __syncthreads();
+    block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
+    for (int d = tid; d < RADIX; d += THREADS)
+      sbase[d] = (u32)seg_row0 + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      if (rd[i] & 0x80000000u) {
+        const u32 d = (rd[i] >> 13) & 0x7ffu;
+        rd[i] = 0x80000000u | (sexcl[d] + wh[d] + (rd[i] & 0x1fffu));  // tile-local sorted slot
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();  // every whist read is done (skeys aliases it); the payload has landed
+#pragma unroll
+    for (int i = 0; i < IPT; ++i)
+      if (rd[i] & 0x80000000u) skeys[rd[i] & 0x1fffu] = key[i];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      u32 pv[IPT];
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) pv[i] = spay[w * TILE + toff + i * 32];
+      __syncthreads();  // this word's row-order slots are all read
+#pragma unroll
+      for (int i = 0; i < IPT; ++i)
+        if (rd[i] & 0x80000000u) spay[w * TILE + (rd[i] & 0x1fffu)] = pv[i];
+    }
+    __syncthreads();
+
+    K* kout = (K*)a.keys_out;
+    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+    const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
+    const bool plain = !a.raw_out && !a.reverse;
+    if (full) {
+#pragma unroll
+      for (int i0 = 0; i0 < IPT; i0 += 8) {
+        K kk[8];
+        u32 gg[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const u32 j = (i0 + i) * THREADS + tid;
+          kk[i] = skeys[j];
+          gg[i] = sbase[(u32)(kk[i] >> a.shift) & mask] + j;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const u32 j = (i0 + i) * THREADS + tid;
+          if (gg[i] - row0 >= span) {
+            atomicOr(a.err, DERR_BOUNDS);
+            continue;
+          }
+          u64 g = gg[i];
+          if (plain) {
+            kout[g] = kk[i];
+          } else {
+            if (a.reverse) g = a.n - 1 - g;
+            if (rsz) {
+              const u64 v = untransform_int(a.raw_dtype, a.raw_flags, (u64)kk[i] + a.raw_tmin);
+              if (rsz == 4) ((u32*)a.raw_out)[g] = (u32)v;
+              else if (rsz == 8) ((u64*)a.raw_out)[g] = v;
+              else store_raw(a.raw_out, a.raw_dtype, g, v);
+            } else {
+              kout[g] = kk[i];
+            }
+          }
+          if (NW >= 2 && a.vout64) {
+            a.vout64[g] = (unsigned long long)spay[j] | ((unsigned long long)spay[TILE + j] << 32);
+#pragma unroll
+            for (int w = 2; w < NW; ++w) a.vout[w][g] = spay[w * TILE + j];
+          } else {
+#pragma unroll
+            for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + j];
+          }
+        }
+      }
+    } else {
+      for (u32 j = tid; j < tile_n; j += THREADS) {
+        const K k = skeys[j];
+        const u32 g32 = sbase[(u32)(k >> a.shift) & mask] + j;
+        if (g32 - row0 >= span) {
+          atomicOr(a.err, DERR_BOUNDS);
+          continue;
+        }
+        u64 g = g32;
+        if (a.reverse) g = a.n - 1 - g;
+        if (a.raw_out) store_raw(a.raw_out, a.raw_dtype, g, untransform_int(a.raw_dtype, a.raw_flags, (u64)k + a.raw_tmin));
+        else kout[g] = k;
+        if (NW >= 2 && a.vout64) {
+          a.vout64[g] = (unsigned long long)spay[j] | ((unsigned long long)spay[TILE + j] << 32);
+#pragma unroll
+          for (int w = 2; w < NW; ++w) a.vout[w][g] = spay[w * TILE + j];
+        } else {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) a.vout[w][g] = spay[w * TILE + j];
+        }
+      }
+    }
+    if (a.status_next)
+      for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
+    return;
   }
 
   // Digit counts first: per-warp histograms by shared-memory atomics (order
@@ -1397,19 +1539,21 @@ inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b, int words = 1) {
   b.status[1] = ar.take<u32>(b.status_words);
 }
 
-template <typename K, int RB, int FM, int NW = 1>
+template <typename K, int RB, int FM, int NW = 1, bool TP = false>
 inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles = 0) {
   constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
+  if (TP && (!a.tile_base || a.digit_mode != DIG_BITS || a.segmented))
+    return fail(JFX_ERR_ARG, "two-phase pass without tile bases or with non-bit digits");
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FM, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FM, NW, TP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::SMEM));
     attr_set = true;
   }
   int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
   const long t = timing_begin(s);
-  k_onesweep<K, RB, FM, NW><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
+  k_onesweep<K, RB, FM, NW, TP><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
   if (t >= 0) {
     // algorithmic bytes: the first pass reads the key columns and writes
     // key + row id; later passes read and write key + row id
@@ -1623,12 +1767,13 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       a.ntiles = tiles;
       a.status = nullptr;
     }
+    const bool tp = a.tile_base != nullptr;  // two-phase (plain bit digits, not segmented)
     if (p == 0 && int1) {
-      JFX_TRY((launch_pass<K, RB, 1, NW>(a, n, s)));
+      JFX_TRY(tp ? (launch_pass<K, RB, 1, NW, true>(a, n, s)) : (launch_pass<K, RB, 1, NW, false>(a, n, s)));
     } else if (p == 0) {
-      JFX_TRY((launch_pass<K, RB, 2, NW>(a, n, s)));
+      JFX_TRY(tp ? (launch_pass<K, RB, 2, NW, true>(a, n, s)) : (launch_pass<K, RB, 2, NW, false>(a, n, s)));
     } else {
-      JFX_TRY((launch_pass<K, RB, 0, NW>(a, n, s)));
+      JFX_TRY(tp ? (launch_pass<K, RB, 0, NW, true>(a, n, s)) : (launch_pass<K, RB, 0, NW, false>(a, n, s)));
     }
   }
   rq.keys_result = out_keys;
