@@ -161,6 +161,9 @@ struct PassArgs {
   // pass then needs no look-back and takes tile ids from blockIdx
   const u32* tile_base;
   u64 ntiles;
+  // two-phase pass: [RADIX] global start of each digit (tile_base holds the
+  // prefix over earlier tiles only)
+  const u32* digit_starts;
 };
 
 __device__ __forceinline__ u32 fmix32(u32 h) {
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     __syncthreads();
     block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
     for (int d = tid; d < RADIX; d += THREADS)
-      sbase[d] = (u32)seg_row0 + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
+      sbase[d] = (u32)seg_row0 + a.digit_starts[d] + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
       if (rd[i] & 0x80000000u) {
@@ -1165,8 +1168,13 @@ template <int T>
 constexpr size_t tile_scan_smem() { return (size_t)(T * kTileScanPer + T * kTileScanPer / 32) * sizeof(u32); }
 __device__ __forceinline__ u32 tile_scan_slot(u32 i) { return i + (i >> 5); }
 
+// With bin_base null the bases start at 0, the row's total goes to
+// totals[d], and the last CTA to finish (counted on *done, which it resets)
+// writes starts[d] = the sum of the totals below d: the two-phase passes add
+// these digit starts themselves, so no histogram of the keys is needed.
 template <int T>
-__global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base) {
+__global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base,
+                                                 u32* totals, u32* starts, u32* done) {
   constexpr int PER = kTileScanPer, CH = T * PER;
   static_assert(T % 32 == 0 && T <= 1024, "warps of a block");
   extern __shared__ u32 buf[];  // [CH + CH / 32]
@@ -1174,7 +1182,7 @@ __global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, c
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const u32* row = counts + (u64)blockIdx.x * tiles;
   u32* out = base + (u64)blockIdx.x * tiles;
-  u32 carry = bin_base[blockIdx.x];
+  u32 carry = bin_base ? bin_base[blockIdx.x] : 0u;
   for (u64 c0 = 0; c0 < tiles; c0 += CH) {
     const u32 m = (u32)min((u64)CH, tiles - c0);
 #pragma unroll
@@ -1227,6 +1235,51 @@ __global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, c
     carry = wsum[0];
     __syncthreads();  // wsum and buf are rewritten next round
   }
+  if (bin_base) return;
+  __shared__ u32 s_last;
+  if (tid == 0) {
+    totals[blockIdx.x] = carry;
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // exclusive scan of the gridDim.x (<= 2048) totals: PER2 consecutive per thread
+  const u32 R = gridDim.x, PER2 = (R + T - 1) / T;
+  u32 sum = 0;
+  for (u32 k = 0; k < PER2; ++k) {
+    const u32 d = tid * PER2 + k;
+    if (d < R) sum += __ldcg(totals + d);
+  }
+  u32 x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const u32 w = lane < T / 32 ? wsum[lane] : 0u;
+    u32 z = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= o) z += y;
+    }
+    if (lane < T / 32) wsum[lane] = z - w;
+  }
+  __syncthreads();
+  u32 run = wsum[warp] + x - sum;
+  for (u32 k = 0; k < PER2; ++k) {
+    const u32 d = tid * PER2 + k;
+    if (d < R) {
+      starts[d] = run;
+      run += __ldcg(totals + d);
+    }
+  }
+  if (tid == 0) *done = 0u;
 }
 
 // ---------------------------------------------------------------- min/max ---
@@ -1503,6 +1556,8 @@ struct SortBuffers {
   u32* counters;   // [8]
   u32* status[2];  // [tiles][RADIX] ping-pong look-back words
   u64 status_words;
+  u32* totals;     // [2048] digit totals of the current two-phase pass
+  u32* starts;     // [2048] their exclusive scan: global start of each digit
 };
 
 inline u64 max_status_words(u64 n) {
@@ -1514,11 +1569,14 @@ inline u64 max_status_words(u64 n) {
   return std::max(std::max(w8, w9), std::max(w10, w11));
 }
 
-inline int launch_tile_scan(int radix, const u32* counts, u64 tiles, const u32* bin_base, u32* base, cudaStream_t s) {
+inline int launch_tile_scan(int radix, const u32* counts, u64 tiles, const u32* bin_base, u32* base, u32* totals,
+                            u32* starts, u32* done, cudaStream_t s) {
   if (tiles >= 32768)
-    k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base), note_launch();
+    k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base, totals, starts, done),
+        note_launch();
   else
-    k_tile_scan<256><<<radix, 256, tile_scan_smem<256>(), s>>>(counts, tiles, bin_base, base), note_launch();
+    k_tile_scan<256><<<radix, 256, tile_scan_smem<256>(), s>>>(counts, tiles, bin_base, base, totals, starts, done),
+        note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }
@@ -1537,6 +1595,8 @@ inline void take_sort_buffers(Arena& ar, u64 n, SortBuffers& b, int words = 1) {
   b.status_words = max_status_words(n);
   b.status[0] = ar.take<u32>(b.status_words);
   b.status[1] = ar.take<u32>(b.status_words);
+  b.totals = ar.take<u32>(2048);
+  b.starts = ar.take<u32>(2048);
 }
 
 template <typename K, int RB, int FM, int NW = 1, bool TP = false>
@@ -1681,7 +1741,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
         hi.tmin2 = rq.pack.c[1].tmin;
         hi.kshift2 = rq.pack.c[1].shift;
       }
-      hi.npass = npass;
+      hi.npass = first_two_phase ? 0 : npass;  // two-phase passes take their digit starts from the tile counts
       for (int p = 0; p < 8; ++p) {
         hi.shift[p] = shift[p];
         hi.mask[p] = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
@@ -1704,11 +1764,13 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     }
     JFX_CUDA(cudaGetLastError());
   }
-  k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
-  JFX_CUDA(cudaGetLastError());
+  if (!first_two_phase) {
+    k_hist_scan<RB><<<npass, 1024, 0, s>>>(b.hist, b.base), note_launch();
+    JFX_CUDA(cudaGetLastError());
+  }
 
   if (first_two_phase) {
-    JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, b.base, b.status[0], s));
+    JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, nullptr, b.status[0], b.totals, b.starts, b.counters + 63, s));
     JFX_CUDA(cudaGetLastError());
   }
   u32* out_vals[kMaxWords];
@@ -1754,9 +1816,11 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       const u32 mask_p = width[p] >= 32 ? 0xffffffffu : ((1u << width[p]) - 1u);
       k_tile_count<K, RB, NW><<<(unsigned)tiles, 256, 0, s>>>((const K*)a.keys_in, n, shift[p], mask_p, b.status[1],
                                                            tiles), note_launch();
-      JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, a.bin_base, b.status[0], s));
+      JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, nullptr, b.status[0], b.totals, b.starts, b.counters + 63,
+                               s));
       JFX_CUDA(cudaGetLastError());
       a.tile_base = b.status[0];
+      a.digit_starts = b.starts;
       a.ntiles = tiles;
       a.status = nullptr;
       a.status_next = nullptr;
@@ -1764,6 +1828,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
     if (two_phase && p == 0) a.status_next = nullptr;
     if (first_two_phase && p == 0) {
       a.tile_base = b.status[0];
+      a.digit_starts = b.starts;
       a.ntiles = tiles;
       a.status = nullptr;
     }
