@@ -1062,7 +1062,16 @@ static int join_expand(const JoinPlan* jp, int32_t* left_idx_out, int32_t* right
   const u32* pB = swap ? jp->pL : jp->pR;
   int32_t* a_out = swap ? right_idx_out : left_idx_out;
   int32_t* b_out = swap ? left_idx_out : right_idx_out;
-  if (jp->unique) {
+  bool carried_only = pay.n > 0 && !pay.gathered && ko.fast_size && !a_out && !b_out;
+  for (int k = 0; k < pay.n && carried_only; ++k)
+    carried_only = pay.cw0[k] && pay.kind[k] >= PK_SAME4 && pay.kind[k] <= PK_U64_F32;
+  if (jp->unique && carried_only) {
+    const int g = grid_for(na, 256);
+    if (jp->key64)
+      k_join_expand_unique_carried<u64><<<g, 256, 0, s>>>(na, jp->lo, (const u64*)skA, ko, pay), note_launch();
+    else
+      k_join_expand_unique_carried<u32><<<g, 256, 0, s>>>(na, jp->lo, (const u32*)skA, ko, pay), note_launch();
+  } else if (jp->unique) {
     const int g = grid_for(na, 256);
     if (jp->key64)
       k_join_expand_unique<u64><<<g, 256, 0, s>>>(na, jp->lo, pA, pB, (const u64*)skA, a_out, b_out, ko, pay), note_launch();
@@ -1320,7 +1329,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   JFX_CUDA(cudaMemsetAsync(l.last, 0, kLeaves * sizeof(u32), s));
   JFX_CUDA(cudaMemsetAsync(l.flags, 0x01, 8 * sizeof(u32), s));
   k_leaf_bounds<<<g, 256, 0, s>>>(l.ssorted, l.s, l.model, l.first, l.last), note_launch();
-  k_leaf_fit<<<kLeaves * 32 / 256, 256, 0, s>>>(l.ssorted, l.first, l.last, l.fit), note_launch();
+  k_leaf_fit<<<kLeaves, 256, 0, s>>>(l.ssorted, l.first, l.last, l.fit), note_launch();
   // predicted positions range over [0, 4n): finer than one slot per row, so
   // distinct keys share a position less often
   const u64 npos = 4 * N;

@@ -566,6 +566,69 @@ __global__ void __launch_bounds__(256) k_join_expand_unique(u64 na, const u32* l
   }
 }
 
+// k_join_expand_unique for its common form: every payload carried through
+// the sorts (no row ids needed), one 4/8-byte integer key column, and a
+// conversion without per-element dtype dispatch.  Loads and stores only what
+// that form needs, in few registers, so more warps hide the load latency.
+template <typename K>
+__global__ void __launch_bounds__(256) k_join_expand_unique_carried(u64 na, const u32* lo, const K* skA,
+                                                                    JoinKeyOut ko, JoinPayloads pay) {
+  constexpr int U = 4;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  const ColDesc& kc = ko.c[0];
+  const u64 kmask = kc.bits >= 64 ? ~0ull : ((1ull << kc.bits) - 1ull);
+  for (u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; i0 < na; i0 += stride * U) {
+    u32 l[U];
+    K kk[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const u64 i = i0 + (u64)u * stride;
+      if (i < na) {
+        l[u] = __ldg(lo + i);
+        kk[u] = __ldg(skA + i);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const u64 i = i0 + (u64)u * stride;
+      if (i >= na) break;
+      const u64 field = (((u64)kk[u] >> kc.shift) & kmask) + kc.tmin;
+      if (ko.fast_size == 8) ((u64*)ko.out[0])[i] = field ^ ko.fast_flip;
+      else ((u32*)ko.out[0])[i] = (u32)field ^ (u32)ko.fast_flip;
+    }
+    for (int k = 0; k < pay.n; ++k) {
+      const bool right = pay.side[k] != pay.swap;
+      const u32* w0 = pay.cw0[k];
+      const u32* w1 = pay.cw1[k];
+      u64 raw[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 i = i0 + (u64)u * stride;
+        raw[u] = 0ull;
+        if (i < na) {
+          const u64 r = right ? (u64)l[u] : i;
+          raw[u] = (u64)__ldg(w0 + r) | (w1 ? (u64)__ldg(w1 + r) << 32 : 0ull);
+        }
+      }
+      void* out = pay.out[k];
+      const int kind = pay.kind[k];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const u64 i = i0 + (u64)u * stride;
+        if (i >= na) break;
+        switch (kind) {
+          case PK_SAME4: ((u32*)out)[i] = (u32)raw[u]; break;
+          case PK_SAME8: ((u64*)out)[i] = raw[u]; break;
+          case PK_I32_F32: ((float*)out)[i] = (float)(int)raw[u]; break;
+          case PK_U32_F32: ((float*)out)[i] = (float)(u32)raw[u]; break;
+          case PK_I64_F32: ((float*)out)[i] = (float)(long long)raw[u]; break;
+          default: ((float*)out)[i] = (float)raw[u]; break;  // PK_U64_F32
+        }
+      }
+    }
+  }
+}
+
 // left / right join: one output per sorted A row, first match in B or -1.
 template <typename K>
 __global__ void __launch_bounds__(256) k_join_expand_first(u64 na, const u32* lo, const u32* cnt,

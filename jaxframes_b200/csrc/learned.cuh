@@ -82,31 +82,43 @@ __global__ void k_leaf_bounds(const u64* sx, u64 s, const ModelRef* mp, u32* fir
   }
 }
 
-// Least-squares line rank ~ base + slope * (x - x0) per leaf (a warp per leaf).
+// Sum of v over the block (256 threads); every thread gets the total.
+__device__ __forceinline__ double block_sum256(double v, double* red) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // red is free (an earlier call's readers are done)
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) t += red[w];
+  return t;
+}
+
+// Least-squares line rank ~ base + slope * (x - x0) per leaf, one block per
+// leaf: the leaves' sample counts are very uneven on skewed keys (a leaf can
+// hold a tenth of the sample when many keys are equal).
 __global__ void __launch_bounds__(256) k_leaf_fit(const u64* sx, const u32* first, const u32* last, double* fit) {
-  const int l = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (l >= kLeaves) return;
+  __shared__ double red[8];
+  const int l = blockIdx.x;
   const u32 s0 = first[l];
   if (s0 == 0xffffffffu) return;
   const u32 e0 = last[l];
   const u64 x0 = sx[s0];
   const double cnt = (double)(e0 - s0);
   double sd = 0;
-  for (u32 i = s0 + lane; i < e0; i += 32) sd += (double)(sx[i] - x0);
-  for (int o = 16; o; o >>= 1) sd += __shfl_xor_sync(0xffffffffu, sd, o);
+  for (u32 i = s0 + threadIdx.x; i < e0; i += 256) sd += (double)(sx[i] - x0);
+  sd = block_sum256(sd, red);
   const double md = sd / cnt, mr = 0.5 * ((double)s0 + (double)(e0 - 1));
   double c = 0, v = 0;
-  for (u32 i = s0 + lane; i < e0; i += 32) {
+  for (u32 i = s0 + threadIdx.x; i < e0; i += 256) {
     const double dd = (double)(sx[i] - x0) - md;
     c += dd * ((double)i - mr);
     v += dd * dd;
   }
-  for (int o = 16; o; o >>= 1) {
-    c += __shfl_xor_sync(0xffffffffu, c, o);
-    v += __shfl_xor_sync(0xffffffffu, v, o);
-  }
-  if (lane == 0) {
+  c = block_sum256(c, red);
+  v = block_sum256(v, red);
+  if (threadIdx.x == 0) {
     double slope = v > 0 ? c / v : 0.0;
     if (!(slope >= 0)) slope = 0;
     fit[2 * l] = slope;
@@ -355,29 +367,42 @@ __global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals,
   u64 pos = t1;
   u64 e = n;
   bool ended = false;
-  while (pos < n) {
-    const u64 q = pos + lane;
-    const bool in = q < n;
-    const u64 k = in ? keys[q] : 0;
-    const bool same = in && spos[q] == p0;
-    const u32 bs = __ballot_sync(0xffffffffu, same);
-    const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
-    const u64 km = lane == 0 ? prev_key : kp;
-    const u32 run_lanes = ~bs ? (u32)(__ffs(~bs) - 1) : 32u;
-    const bool mine = (u32)lane < run_lanes;
-    inv |= __ballot_sync(0xffffffffu, mine && km > k) != 0;
-    distinct |= __ballot_sync(0xffffffffu, mine && k != k0) != 0;
-    if (run_lanes < 32) {
-      e = pos + run_lanes;
-      ended = true;
-      break;
+  constexpr int CH = 8;  // 32-key chunks loaded per round trip
+  bool done = false;
+  while (pos < n && !done) {
+    u64 kc[CH];
+    bool sc[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const u64 q = pos + 32 * c + lane;
+      kc[c] = q < n ? keys[q] : 0;
+      sc[c] = q < n && spos[q] == p0;
     }
-    prev_key = __shfl_sync(0xffffffffu, k, 31);
-    pos += 32;
-    const u64 scanned = pos - (base + i);
-    if ((!distinct && !inv && scanned > (u64)kFixMaxRun) || scanned > (u64)kFixLongMax) {
-      e = pos;
-      break;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      if (done || pos >= n) break;
+      const u64 k = kc[c];
+      const u32 bs = __ballot_sync(0xffffffffu, sc[c]);
+      const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
+      const u64 km = lane == 0 ? prev_key : kp;
+      const u32 run_lanes = ~bs ? (u32)(__ffs(~bs) - 1) : 32u;
+      const bool mine = (u32)lane < run_lanes;
+      inv |= __ballot_sync(0xffffffffu, mine && km > k) != 0;
+      distinct |= __ballot_sync(0xffffffffu, mine && k != k0) != 0;
+      if (run_lanes < 32) {
+        e = pos + run_lanes;
+        ended = true;
+        done = true;
+        break;
+      }
+      prev_key = __shfl_sync(0xffffffffu, k, 31);
+      pos += 32;
+      const u64 scanned = pos - (base + i);
+      if ((!distinct && !inv && scanned > (u64)kFixMaxRun) || scanned > (u64)kFixLongMax) {
+        e = pos;
+        done = true;
+        break;
+      }
     }
   }
   if (pos >= n) ended = true;

@@ -295,6 +295,30 @@ def test_join_c2_like_payloads(P):
         np.testing.assert_array_equal(g, eout[c])
 
 
+@pytest.mark.parametrize("kdt", [np.int32, np.int64, np.uint32, np.uint64])
+def test_join_every_row_matches_once_payload_kinds(P, kdt):
+    """Every left row matches exactly one right row (the expand that writes
+    output i from sorted left row i), all payloads carried through the sorts,
+    one integer key column of each width and signedness: each payload
+    conversion (4- and 8-byte copies, int32/uint32/int64/uint64 to float32)."""
+    rng = np.random.default_rng(19 + np.dtype(kdt).itemsize)
+    nl, nr = 300_001, 120_000
+    lk = rng.integers(0, nr, nl).astype(kdt)
+    rk = rng.permutation(nr).astype(kdt)
+    lv = {"a": rng.standard_normal(nl), "b": rng.integers(0, 2**32, nl, dtype=np.uint64).astype(np.uint32),
+          "c": rng.integers(-2**31, 2**31, nl).astype(np.int32)}
+    rv = {"d": rng.integers(-2**62, 2**62, nr), "e": rng.integers(0, 2**63, nr, dtype=np.uint64)}
+    mk, out = P.sort_merge_join(lk, lv, rk, rv, "inner")
+    emk, eout, _, _ = O.sort_merge_join(lk, lv, rk, rv, "inner")
+    np.testing.assert_array_equal(_np(mk), emk)
+    assert _np(mk).dtype == emk.dtype
+    assert set(out) == set(eout)
+    for c in eout:
+        g = _np(out[c])
+        assert g.dtype == eout[c].dtype, c
+        np.testing.assert_array_equal(g, eout[c], err_msg=c)
+
+
 @pytest.mark.parametrize("how", ["inner", "left", "right"])
 def test_join_many_payloads_partial_matches(P, how):
     """Unique right keys with half the left keys unmatched (the general expand,
