@@ -527,7 +527,16 @@ __global__ void __launch_bounds__(kFixMedThreads) k_fix_medium(u64* keys, u32* v
         const u32 j = j0 + lane;
         const bool in = j < w1;
         const u32 d = in ? (u32)(((src[j] - mn) >> sh) & 255u) : 256u;
-        const u32 peers = __match_any_sync(0xffffffffu, d);
+        // lanes with the same digit: one ballot per digit bit (faster than
+        // match.any here); lanes past the segment end form their own group
+        u32 peers = __ballot_sync(0xffffffffu, in);
+        if (!in) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const u32 bit = (d >> b) & 1u;
+          const u32 bb = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? bb : ~bb;
+        }
         const u32 prior = in ? wh[warp * 256 + d] : 0u;
         const u32 dst_i = prior + __popc(peers & lt);
         __syncwarp();
