@@ -255,12 +255,13 @@ static int plain_sort_u64(const u64* keys, u64 n, u64* sorted_out, u32* perm_out
   JFX_TRY(build_pack(&col, 1, 0u, false, pd));
   KeyPlan kp;
   kp.pack = pd;
-  JFX_TRY(plan_keys(kp, n, c.mm, s));
+  JFX_TRY(plan_keys(kp, n, c.mm, s, nullptr, b.status[1]));
   RadixRequest rq;
   rq.pack = kp.pack;
   rq.total_bits = kp.total_bits;
   rq.key64 = kp.total_bits > 32;
   rq.perm_out = perm_out;
+  rq.pre_counts = kp.pre_counts;
   if (kp.total_bits > 0) {
     rq.raw_out = sorted_out;
     rq.raw_dtype = JFX_U64;
@@ -506,13 +507,14 @@ int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   KeyPlan kp;
   kp.pack = pd;
-  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s));
+  JFX_TRY(plan_keys(kp, (u64)n, c.mm, s, nullptr, b.status[1]));
   RadixRequest rq;
   rq.pack = kp.pack;
   rq.total_bits = kp.total_bits;
   rq.key64 = kp.total_bits > 32;
   rq.reverse = !ascending;
   rq.perm_out = (u32*)perm_out;
+  rq.pre_counts = kp.pre_counts;
   const bool int_keys = !dtype_is_float(key->dtype);
   if (sorted_keys_out && int_keys && kp.total_bits > 0) {
     rq.raw_out = sorted_keys_out;
@@ -848,6 +850,8 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
   JFX_TRY(build_pack(left_keys, ncols, flags, false, pl));
   JFX_TRY(build_pack(right_keys, ncols, flags, false, pr));
   // shared packing: min and max of every column over both sides
+  // (the sides' first-pass tile counts are left to their sorts, which run on
+  // two streams: counting them here, before the fork, lengthened the join)
   JFX_TRY(launch_minmax(pl, (u64)nl, c.mm, s));
   JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2 * kMaxCols, s));
   u64* host = g_host.get();

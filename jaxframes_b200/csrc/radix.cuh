@@ -1172,15 +1172,17 @@ __device__ __forceinline__ u32 tile_scan_slot(u32 i) { return i + (i >> 5); }
 // totals[d], and the last CTA to finish (counted on *done, which it resets)
 // writes starts[d] = the sum of the totals below d: the two-phase passes add
 // these digit starts themselves, so no histogram of the keys is needed.
+// rot: digit d's counts are row (d + rot) mod RADIX of `counts` (first-pass
+// counts taken from the min/max pass, rotated by the minimum's low byte).
 template <int T>
 __global__ void __launch_bounds__(T) k_tile_scan(const u32* counts, u64 tiles, const u32* bin_base, u32* base,
-                                                 u32* totals, u32* starts, u32* done) {
+                                                 u32* totals, u32* starts, u32* done, u32 rot) {
   constexpr int PER = kTileScanPer, CH = T * PER;
   static_assert(T % 32 == 0 && T <= 1024, "warps of a block");
   extern __shared__ u32 buf[];  // [CH + CH / 32]
   __shared__ u32 wsum[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const u32* row = counts + (u64)blockIdx.x * tiles;
+  const u32* row = counts + (u64)((blockIdx.x + rot) & (gridDim.x - 1)) * tiles;
   u32* out = base + (u64)blockIdx.x * tiles;
   u32 carry = bin_base ? bin_base[blockIdx.x] : 0u;
   for (u64 c0 = 0; c0 < tiles; c0 += CH) {
@@ -1404,6 +1406,71 @@ __global__ void __launch_bounds__(256) k_minmax_int(const T* col, u64 n, u64 fli
   }
 }
 
+// k_minmax_int that also counts, per 2048-row tile, the low byte of every
+// value (digit-major [256][tiles]).  Once the minimum is known, the first
+// 8-bit radix pass's tile counts are these counts rotated by the minimum's
+// low byte (the packed key is value - min, and the sign flip leaves the low
+// byte alone), so that pass needs no separate counting read of the column.
+constexpr int kPreTile = 2048;
+template <typename T>
+__global__ void __launch_bounds__(256) k_minmax_int_tiles(const T* col, u64 n, u64 flip, u64* out, u32* counts,
+                                                          u64 tiles) {
+  constexpr int NH = 8, IPT = kPreTile / 256;  // one histogram per warp
+  __shared__ u32 h[NH][256];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < NH * 256; i += 256) (&h[0][0])[i] = 0u;
+  __syncthreads();
+  u64 mn = ~0ull, mx = 0ull;
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const u64 base = t * kPreTile;
+    const u32 tn = (u32)min((u64)kPreTile, n - base);
+    T raw[IPT];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 r = i * 256 + tid;
+      raw[i] = r < tn ? __ldg(col + base + r) : (T)0;
+    }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      if (i * 256 + tid >= tn) break;
+      const u64 v = (u64)raw[i] ^ flip;
+      mn = v < mn ? v : mn;
+      mx = v > mx ? v : mx;
+      atomicAdd(&h[warp][(u32)raw[i] & 255u], 1u);
+    }
+    __syncthreads();
+    u32 c = 0;
+#pragma unroll
+    for (int q = 0; q < NH; ++q) {
+      c += h[q][tid];
+      h[q][tid] = 0u;
+    }
+    counts[(u64)tid * tiles + t] = c;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const u64 a2 = __shfl_xor_sync(0xffffffffu, mn, o);
+    const u64 b2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mn = a2 < mn ? a2 : mn;
+    mx = b2 > mx ? b2 : mx;
+  }
+  __shared__ u64 smn[8], smx[8];
+  if (lane == 0) {
+    smn[warp] = mn;
+    smx[warp] = mx;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < 8; ++w) {
+      mn = smn[w] < mn ? smn[w] : mn;
+      mx = smx[w] > mx ? smx[w] : mx;
+    }
+    atomicMin((unsigned long long*)&out[0], (unsigned long long)mn);
+    atomicMax((unsigned long long*)&out[1], (unsigned long long)mx);
+  }
+}
+
 __global__ void k_init_minmax(u64* out, int ncols) {
   int j = threadIdx.x;
   if (j < ncols) {
@@ -1449,6 +1516,7 @@ struct KeyPlan {
   PackDesc pack;
   int total_bits = 0;
   u64 tmax[kMaxCols];
+  const u32* pre_counts = nullptr;  // low-byte tile counts of the min/max pass, if written
 };
 
 // Fill `cols` from jfx_column descriptors (validates dtypes).
@@ -1469,7 +1537,12 @@ inline int build_pack(const jfx_column* in, int ncols, u32 extra_flags, bool all
   return JFX_OK;
 }
 
-inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s) {
+// tile_counts (optional, [256][ceil(n / 2048)] words): for one plain integer
+// key column, also the low-byte counts of k_minmax_int_tiles; *counted says
+// whether they were written.
+inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s, u32* tile_counts = nullptr,
+                         bool* counted = nullptr) {
+  if (counted) *counted = false;
   k_init_minmax<<<1, 32, 0, s>>>(dev_out, pd.ncols), note_launch();
   if (n) {
     int grid = (int)std::min<u64>((n + 255) / 256, (u64)device_sm_count() * 8);
@@ -1482,7 +1555,17 @@ inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s
       const int dt = pd.c[j].dtype;
       all_int &= !(pd.c[j].flags & CF_DESC) && (dt == JFX_I32 || dt == JFX_I64 || dt == JFX_U32 || dt == JFX_U64);
     }
-    if (int_key && (d0 == JFX_I64 || d0 == JFX_U64))
+    if (int_key && tile_counts) {
+      const u64 tiles = (n + kPreTile - 1) / kPreTile;
+      const int tg = (int)std::min<u64>(tiles, (u64)device_sm_count() * 8);
+      if (d0 == JFX_I64 || d0 == JFX_U64)
+        k_minmax_int_tiles<u64><<<tg, 256, 0, s>>>((const u64*)pd.c[0].ptr, n, flip, dev_out, tile_counts, tiles),
+            note_launch();
+      else
+        k_minmax_int_tiles<u32><<<tg, 256, 0, s>>>((const u32*)pd.c[0].ptr, n, flip, dev_out, tile_counts, tiles),
+            note_launch();
+      if (counted) *counted = true;
+    } else if (int_key && (d0 == JFX_I64 || d0 == JFX_U64))
       k_minmax_int<u64><<<grid, 256, 0, s>>>((const u64*)pd.c[0].ptr, n, flip, dev_out), note_launch();
     else if (int_key)
       k_minmax_int<u32><<<grid, 256, 0, s>>>((const u32*)pd.c[0].ptr, n, flip, dev_out), note_launch();
@@ -1507,7 +1590,10 @@ inline int launch_minmax(const PackDesc& pd, u64 n, u64* dev_out, cudaStream_t s
 // fields.  One stream synchronisation.
 // host: 2 * ncols words of host memory for the read-back (null: the pinned
 // per-thread buffer).
-inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s, u64* host = nullptr) {
+// tile_counts: optional [256][ceil(n / 2048)] words for the low-byte tile
+// counts of a plain integer key column (kp.pre_counts is set when written).
+inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s, u64* host = nullptr,
+                     u32* tile_counts = nullptr) {
   PackDesc& pd = kp.pack;
   if (!host) host = g_host.get();
   if (!host) return fail(JFX_ERR_CUDA, "cudaMallocHost failed");
@@ -1527,7 +1613,9 @@ inline int plan_keys(KeyPlan& kp, u64 n, u64* dev_scratch, cudaStream_t s, u64* 
         pd.c[j].desc_max = raw_max;
       }
   }
-  JFX_TRY(launch_minmax(pd, n, dev_scratch, s));
+  bool counted = false;
+  JFX_TRY(launch_minmax(pd, n, dev_scratch, s, tile_counts, &counted));
+  kp.pre_counts = counted ? tile_counts : nullptr;
   JFX_CUDA(cudaMemcpyAsync(host, dev_scratch, 2 * pd.ncols * sizeof(u64), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaStreamSynchronize(s));
   int shift = 0;
@@ -1570,13 +1658,13 @@ inline u64 max_status_words(u64 n) {
 }
 
 inline int launch_tile_scan(int radix, const u32* counts, u64 tiles, const u32* bin_base, u32* base, u32* totals,
-                            u32* starts, u32* done, cudaStream_t s) {
+                            u32* starts, u32* done, cudaStream_t s, u32 rot = 0) {
   if (tiles >= 32768)
-    k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base, totals, starts, done),
-        note_launch();
+    k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base, totals, starts, done,
+                                                                rot), note_launch();
   else
-    k_tile_scan<256><<<radix, 256, tile_scan_smem<256>(), s>>>(counts, tiles, bin_base, base, totals, starts, done),
-        note_launch();
+    k_tile_scan<256><<<radix, 256, tile_scan_smem<256>(), s>>>(counts, tiles, bin_base, base, totals, starts, done,
+                                                              rot), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }
@@ -1655,6 +1743,10 @@ struct RadixRequest {
   u64 raw_tmin = 0;
   const ModelRef* model = nullptr;  // DIG_MODEL / KEY_MODEL
   unsigned long long* vout64 = nullptr;  // last pass: words 0 and 1 as one u64
+  // optional: low-byte counts of the single integer key column per 2048-row
+  // tile (k_minmax_int_tiles), used for the first pass when it has 8-bit
+  // digits over 2048-row tiles instead of counting the column again
+  const u32* pre_counts = nullptr;
 };
 
 template <typename K, int RB, int NW>
@@ -1695,6 +1787,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
                        !(rq.pack.c[0].flags & CF_DESC) && plain_int(d0);
   // (a gathered first pass reads its tiles in another order than the column)
   const bool first_two_phase = two_phase && int_key && !rq.gather_idx;
+  // the first pass's tile counts from the min/max pass (one column, 8-bit
+  // first digit at bit 0, 2048-row tiles): no counting kernel at all
+  const bool pre = rq.pre_counts && first_two_phase && RB == 8 && (int)PassLayout<K, RB, NW>::TILE == kPreTile &&
+                   rq.pack.ncols == 1 && rq.pack.c[0].shift == 0 && npass >= 1 && width[0] == 8;
   // the first pass's lean instantiation: one or two plain integer columns of
   // one width, read in order
   const bool int1 = int_key && !rq.gather_idx;
@@ -1755,7 +1851,9 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
         g = (int)std::min<u64>(tiles, (u64)device_sm_count() * 8);
         sm += (size_t)RADIX * sizeof(u32);
       }
-      if (d0 == JFX_I64 || d0 == JFX_U64)
+      if (pre) {
+        // counted by the min/max pass
+      } else if (d0 == JFX_I64 || d0 == JFX_U64)
         k_hist_int<K, u64, RB><<<g, 256, sm, s>>>(hi), note_launch();
       else
         k_hist_int<K, u32, RB><<<g, 256, sm, s>>>(hi), note_launch();
@@ -1770,7 +1868,11 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   }
 
   if (first_two_phase) {
-    JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, nullptr, b.status[0], b.totals, b.starts, b.counters + 63, s));
+    if (pre)
+      JFX_TRY(launch_tile_scan(RADIX, rq.pre_counts, tiles, nullptr, b.status[0], b.totals, b.starts, b.counters + 63, s,
+                               (u32)(rq.pack.c[0].tmin & 255u)));
+    else
+      JFX_TRY(launch_tile_scan(RADIX, b.status[1], tiles, nullptr, b.status[0], b.totals, b.starts, b.counters + 63, s));
     JFX_CUDA(cudaGetLastError());
   }
   u32* out_vals[kMaxWords];
