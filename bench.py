@@ -97,7 +97,7 @@ def c4_keys(nblocks=65_536, block=4096, seed=45):
 # join call, from the ncu capture summarised in
 # profiles/join_10Mx5M_launch_list.md (cold-cache replays; the writes that
 # stay in L2 between passes are not counted).
-ONESWEEP_DRAM_BYTES_PER_LAUNCH = 93.3e6
+ONESWEEP_DRAM_BYTES_PER_LAUNCH = 92.7e6
 
 
 def join_model_bytes(nl, nr, m):
