@@ -852,8 +852,21 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
   // shared packing: min and max of every column over both sides
   // (the sides' first-pass tile counts are left to their sorts, which run on
   // two streams: counting them here, before the fork, lengthened the join)
+  // the right side's min/max runs on the side stream beside the left's
+  SideStream* mss = nullptr;
+  cudaStream_t sm2 = s;
+  if (nl && nr) {
+    JFX_TRY(side_stream(&mss));
+    sm2 = mss->stream;
+    JFX_CUDA(cudaEventRecord(mss->fork, s));
+    JFX_CUDA(cudaStreamWaitEvent(sm2, mss->fork, 0));
+  }
   JFX_TRY(launch_minmax(pl, (u64)nl, c.mm, s));
-  JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2 * kMaxCols, s));
+  JFX_TRY(launch_minmax(pr, (u64)nr, c.mm + 2 * kMaxCols, sm2));
+  if (mss) {
+    JFX_CUDA(cudaEventRecord(mss->join, sm2));
+    JFX_CUDA(cudaStreamWaitEvent(s, mss->join, 0));
+  }
   u64* host = g_host.get();
   JFX_TRY(read_back(c.mm, 4 * kMaxCols * sizeof(u64), host, s));
   int shift = 0;
