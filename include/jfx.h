@@ -259,18 +259,43 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
 int jfx_batch_status(void* workspace, size_t workspace_bytes, void* stream);
 
 /* Tuning of this thread's later calls (no counterpart in the reference): the
- * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width))
- * and whether the passes after the first run in two phases (per-tile digit
+ * widest radix digit per pass (8..11 bits; passes = ceil(key bits / width)),
+ * whether the passes after the first run in two phases (per-tile digit
  * counts and a scan first, then the pass without a look-back; 1, the
- * default) or as single look-back passes (0).  jfx_set_tuning(NULL) restores
- * the defaults.  The autotuner (jaxframes_b200/autotune.py) picks values per
- * key dtype, size and skew. */
+ * default) or as single look-back passes (0), and the bound of every
+ * device-side wait in microseconds (a decoupled look-back that waits longer
+ * on an earlier tile gives up and the call returns JFX_ERR_TIMEOUT; 1..10^7,
+ * default 10^6 = 1 s).  jfx_set_tuning(NULL) restores the defaults.  The
+ * autotuner (jaxframes_b200/autotune.py) picks values per key dtype, size and
+ * skew. */
 typedef struct {
   int32_t max_digit_bits;
   int32_t two_phase;
+  int32_t spin_limit_us;
+  int32_t reserved;
 } jfx_tuning;
 int jfx_set_tuning(const jfx_tuning* t);
 int jfx_get_tuning(jfx_tuning* t);
+
+/* Failure injection for this thread's later calls, to test the error paths
+ * without faulting a GPU (no counterpart in the reference).  All zero (or
+ * jfx_set_fault(NULL)) injects nothing.
+ *   withhold_tile:    >= 1: in every decoupled look-back pass, the tile with
+ *                     that ticket never publishes its counts, so the later
+ *                     tiles' bounded waits run out and the call returns
+ *                     JFX_ERR_TIMEOUT (give a short spin_limit_us);
+ *   learned_fallback: -1 / -2 / -3: jfx_learned_sort takes that fallback (model
+ *                     check failed / run too long / run list full) as if its
+ *                     own check had found it; the output is the plain sort's;
+ *   fail_workspace:   1: every entry point that takes a workspace reports it
+ *                     as too small (JFX_ERR_ALLOC) before launching anything. */
+typedef struct {
+  int32_t withhold_tile;
+  int32_t learned_fallback;
+  int32_t fail_workspace;
+  int32_t reserved;
+} jfx_fault;
+int jfx_set_fault(const jfx_fault* f);
 
 /* Measurement hooks.  No counterpart in the reference, which has no tracing.
  * jfx_launch_count: number of kernels this library has launched so far.

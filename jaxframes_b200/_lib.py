@@ -61,7 +61,13 @@ class AggColumn(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("max_digit_bits", ctypes.c_int32), ("two_phase", ctypes.c_int32)]
+    _fields_ = [("max_digit_bits", ctypes.c_int32), ("two_phase", ctypes.c_int32),
+                ("spin_limit_us", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Fault(ctypes.Structure):
+    _fields_ = [("withhold_tile", ctypes.c_int32), ("learned_fallback", ctypes.c_int32),
+                ("fail_workspace", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class JoinPayload(ctypes.Structure):
@@ -109,6 +115,7 @@ SIGNATURES = {
     "jfx_batch_status": (_INT, [_P, _SIZE, _P]),
     "jfx_set_tuning": (_INT, [ctypes.POINTER(Tuning)]),
     "jfx_get_tuning": (_INT, [ctypes.POINTER(Tuning)]),
+    "jfx_set_fault": (_INT, [ctypes.POINTER(Fault)]),
     "jfx_launch_count": (ctypes.c_uint64, []),
     "jfx_timing_enable": (_INT, [_INT]),
     "jfx_timing_read": (_INT, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I64),

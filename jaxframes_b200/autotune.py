@@ -140,13 +140,14 @@ class Autotuner:
 
 
 @contextlib.contextmanager
-def tuning(max_digit_bits: int | None = None, two_phase: bool | None = None):
+def tuning(max_digit_bits: int | None = None, two_phase: bool | None = None, spin_limit_us: int | None = None):
     """Applies a tuning to this thread's libjfx calls for the block."""
     L = _lib.load_library()
     old = _lib.Tuning()
     _lib.check(L.jfx_get_tuning(ctypes.byref(old)))
     new = _lib.Tuning(old.max_digit_bits if max_digit_bits is None else int(max_digit_bits),
-                      old.two_phase if two_phase is None else int(bool(two_phase)))
+                      old.two_phase if two_phase is None else int(bool(two_phase)),
+                      old.spin_limit_us if spin_limit_us is None else int(spin_limit_us), 0)
     _lib.check(L.jfx_set_tuning(ctypes.byref(new)))
     try:
         yield

@@ -9,6 +9,7 @@ thread_local std::string g_last_error;
 thread_local HostScratch g_host;
 std::atomic<unsigned long long> g_launches{0};
 thread_local Tuning g_tuning;
+thread_local Fault g_fault;
 Timing g_timing;
 
 int device_sm_count() {
@@ -65,9 +66,13 @@ __global__ void k_unpack(const K* sk, u64 n, int dtype, u32 flags, u64 tmin, voi
     store_raw(out, dtype, i, untransform_int(dtype, flags, (u64)sk[i] + tmin));
 }
 
+// out[i] = src[idx[i]] over one array of n rows.  An index outside [0, n)
+// (only after a failed pass, which the call reports) reads nothing.
 __global__ void k_gather_same(const void* src, int dt, const u32* idx, u64 n, void* out) {
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-    store_raw(out, dt, i, load_raw(src, dt, idx[i]));
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u32 r = idx[i];
+    store_raw(out, dt, i, r < n ? load_raw(src, dt, r) : 0ull);
+  }
 }
 
 // ------------------------------------------------------------------ sort ---
@@ -408,8 +413,11 @@ int jfx_set_tuning(const jfx_tuning* t) {
   if (t->max_digit_bits < 8 || t->max_digit_bits > 11)
     return fail(JFX_ERR_ARG, "max_digit_bits must be in [8, 11], got %d", t->max_digit_bits);
   if (t->two_phase != 0 && t->two_phase != 1) return fail(JFX_ERR_ARG, "two_phase must be 0 or 1, got %d", t->two_phase);
+  if (t->spin_limit_us < 1 || t->spin_limit_us > 10000000)
+    return fail(JFX_ERR_ARG, "spin_limit_us must be in [1, 10^7], got %d", t->spin_limit_us);
   g_tuning.max_digit_bits = t->max_digit_bits;
   g_tuning.two_phase = t->two_phase;
+  g_tuning.spin_limit_us = t->spin_limit_us;
   return JFX_OK;
 }
 
@@ -417,6 +425,24 @@ int jfx_get_tuning(jfx_tuning* t) {
   if (!t) return fail(JFX_ERR_ARG, "null pointer");
   t->max_digit_bits = g_tuning.max_digit_bits;
   t->two_phase = g_tuning.two_phase;
+  t->spin_limit_us = g_tuning.spin_limit_us;
+  t->reserved = 0;
+  return JFX_OK;
+}
+
+int jfx_set_fault(const jfx_fault* f) {
+  if (!f) {
+    g_fault = Fault();
+    return JFX_OK;
+  }
+  if (f->withhold_tile < 0) return fail(JFX_ERR_ARG, "withhold_tile must be >= 0, got %d", f->withhold_tile);
+  if (f->learned_fallback != 0 && f->learned_fallback != -1 && f->learned_fallback != -2 && f->learned_fallback != -3)
+    return fail(JFX_ERR_ARG, "learned_fallback must be 0, -1, -2 or -3, got %d", f->learned_fallback);
+  if (f->fail_workspace != 0 && f->fail_workspace != 1)
+    return fail(JFX_ERR_ARG, "fail_workspace must be 0 or 1, got %d", f->fail_workspace);
+  g_fault.withhold_tile = f->withhold_tile;
+  g_fault.learned_fallback = f->learned_fallback;
+  g_fault.fail_workspace = f->fail_workspace;
   return JFX_OK;
 }
 
@@ -446,7 +472,7 @@ int jfx_timing_read(double* total_ms, int64_t* launches, double* algo_bytes) {
   if (algo_bytes) *algo_bytes = bytes;
   return JFX_OK;
 }
-int jfx_version(void) { return 1; }
+int jfx_version(void) { return 2; }
 int jfx_max_rows(void) { return (int)kMaxRows; }
 
 size_t jfx_workspace_size(int kind, int64_t n1, int64_t n2) {
@@ -503,7 +529,7 @@ int jfx_sort(const jfx_column* key, int64_t n, int ascending, int32_t* perm_out,
   Common c;
   SortBuffers b;
   carve_sort(ar, (u64)n, c, b);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   KeyPlan kp;
   kp.pack = pd;
@@ -621,7 +647,7 @@ int jfx_lexsort(const jfx_column* keys, int ncols, int64_t n, int32_t* perm_out,
   SortBuffers b;
   u32* tmp;
   carve_lexsort(ar, (u64)n, c, b, &tmp);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   KeyPlan kp;
   kp.pack = pd;
@@ -734,7 +760,7 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   SortBuffers b;
   GroupBuffers g;
   carve_groupby(ar, (u64)n, nvalues, c, b, g);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   KeyPlan kp;
   kp.pack = pd;
@@ -841,7 +867,7 @@ static int join_prepare(const jfx_column* left_keys, int64_t nl, const jfx_colum
   SortBuffers b, br;
   JoinBuffers j;
   carve_join(ar, (u64)nl, (u64)nr, c, b, br, j);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   // a single key is sorted by ParallelRadixSort (narrow ints keep the
   // reference's unsigned order); several keys are compared for equality only
@@ -1280,7 +1306,7 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
   Common c;
   SortBuffers b;
   carve_partition(ar, (u64)n, c, b);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   RadixRequest rq;
   rq.pack = pd;
@@ -1313,7 +1339,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   SortBuffers b;
   LearnedBuffers l;
   carve_learned(ar, (u64)n, c, b, l);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   const u64 N = (u64)n;
   u64* host = g_host.get();
@@ -1386,11 +1412,8 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   k_fix_check<<<grid_for(l.tiles, 256), 256, 0, s>>>(l.tiles, l.fix), note_launch();
   k_fix_small<<<device_sm_count() * 8, 256, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
   {
-    static bool attr = false;
-    if (!attr) {
-      JFX_CUDA(cudaFuncSetAttribute(k_fix_medium, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFixMediumSmem));
-      attr = true;
-    }
+    static SmemAttr attr;
+    JFX_TRY(ensure_smem(attr, k_fix_medium, kFixMediumSmem));
   }
   k_fix_medium<<<device_sm_count(), kFixMedThreads, kFixMediumSmem, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
   // long runs: the sort's ping-pong buffers are free now and serve as scratch
@@ -1403,10 +1426,14 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   JFX_TRY(check_err_word((u32)host[0]));
   const u32 ok = (u32)host[1];
   const u32* cnts = (const u32*)(host + 2);
-  if (!ok || cnts[2]) {
+  if (!ok || cnts[2] || g_fault.learned_fallback) {
     // model not monotone, or a run the fix-up cannot take: plain radix sort.
     // *learned_used reports why: -1 model check, -2 run too long, -3 list full
-    const int why = !ok ? -1 : (cnts[2] & FIX_LONG_RUN) ? -2 : -3;
+    // (or the fallback jfx_set_fault asked for)
+    const int why = g_fault.learned_fallback ? g_fault.learned_fallback
+                    : !ok                   ? -1
+                    : (cnts[2] & FIX_LONG_RUN) ? -2
+                                              : -3;
     JFX_TRY(plain_sort_u64(keys, N, sorted_keys_out, (u32*)perm_out, b, c, s));
     JFX_TRY(read_back(c.err, sizeof(u32), host, s));
     if (learned_used) *learned_used = why;
@@ -1436,7 +1463,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   Common c;
   BatchBuffers bb;
   carve_batch(ar, (u64)n, (u64)nq, c, bb);
-  if (ar.overflow || !workspace) return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed", workspace_bytes, ar.off);
+  JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
   constexpr int RB = kBatchRB, RADIX = 1 << RB;
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
   // segment tables
@@ -1478,11 +1505,8 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
       h.shift[p] = shift[p];
       h.width[p] = width[p];
     }
-    static bool attr = false;
-    if (!attr) {
-      JFX_CUDA(cudaFuncSetAttribute(k_hist_seg<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * RADIX * 4));
-      attr = true;
-    }
+    static SmemAttr attr;
+    JFX_TRY(ensure_smem(attr, k_hist_seg<RB>, 4 * RADIX * 4));
     k_hist_seg<RB><<<device_sm_count() * 4, 256, npass * RADIX * sizeof(u32), s>>>(h), note_launch();
   }
   k_hist_scan<RB><<<(unsigned)(nq * npass), 1024, 0, s>>>(bb.hist, bb.base), note_launch();

@@ -319,7 +319,8 @@ __device__ __forceinline__ u32 lanemask_gt() {
   return m;
 }
 
-// Upper bound on any device-side spin (decoupled look-back, work queues).
+// Default upper bound on any device-side spin (decoupled look-back); the
+// bound a launch uses comes from the tuning (jfx_tuning.spin_limit_us).
 constexpr u64 kSpinLimitNs = 1000000000ull;  // 1 s
 
 // ---------------------------------------------------------------- arena ---
@@ -352,6 +353,27 @@ __host__ __device__ inline int bit_length(u64 v) {
 
 // Number of SMs of the current device (cached per device).
 int device_sm_count();
+
+// One-time raise of a kernel's dynamic shared-memory limit on each device.
+// CUDA keeps the attribute per device, so a process that calls the library on
+// several devices needs it set on every one; each call site owns one
+// SmemAttr (bit d of `done`: set on device d).  Two threads that race here
+// both set the same value, which is harmless.
+struct SmemAttr {
+  std::atomic<unsigned long long> done[2];
+};
+template <typename Kernel>
+inline int ensure_smem(SmemAttr& a, Kernel* kernel, size_t bytes) {
+  int dev = -1;
+  JFX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(JFX_ERR_ARG, "device ordinal %d out of range", dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  std::atomic<unsigned long long>& w = a.done[dev >> 6];
+  if (w.load(std::memory_order_acquire) & bit) return JFX_OK;
+  JFX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  w.fetch_or(bit, std::memory_order_release);
+  return JFX_OK;
+}
 
 // ------------------------------------------------------------ accounting ---
 // Every kernel launch of the library bumps this counter (jfx_launch_count).

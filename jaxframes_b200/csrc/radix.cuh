@@ -164,6 +164,8 @@ struct PassArgs {
   // two-phase pass: [RADIX] global start of each digit (tile_base holds the
   // prefix over earlier tiles only)
   const u32* digit_starts;
+  u64 spin_ns;        // bound of each look-back wait
+  u32 withhold_tile;  // failure injection: this look-back ticket publishes nothing (0: none)
 };
 
 __device__ __forceinline__ u32 fmix32(u32 h) {
@@ -270,8 +272,8 @@ __device__ __forceinline__ void block_exclusive_scan(u32* data, u32* scratch) {
 }
 
 // Bounded spin on a look-back word until its flag is set.  Returns the word, or
-// ST_ERR after kSpinLimitNs or when another CTA already reported a timeout.
-__device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
+// ST_ERR after limit_ns or when another CTA already reported a timeout.
+__device__ __forceinline__ u32 wait_status(const u32* p, u32* err, u64 limit_ns) {
   u32 v = ld_relaxed(p);
   if (v & 0xC0000000u) return v;
   u64 t0 = globaltimer_ns();
@@ -281,7 +283,7 @@ __device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
     if (spins > 128) __nanosleep(64);
     if ((spins & 255u) == 0) {
       if (ld_relaxed(err) & DERR_TIMEOUT) return ST_ERR;
-      if (globaltimer_ns() - t0 > kSpinLimitNs) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         atomicOr(err, DERR_TIMEOUT);
         return ST_ERR;
       }
@@ -294,7 +296,7 @@ __device__ __forceinline__ u32 wait_status(const u32* p, u32* err) {
 // inclusive word.  A word not yet published is waited on (bounded).
 template <int W>
 __device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 tile0, u32 d, u32 radix,
-                                               u32* err, bool& bad) {
+                                               u32* err, u64 limit_ns, bool& bad) {
   u32 excl = 0;
   long k = (long)tile - 1;  // next predecessor to read; tile0 publishes inclusive sums
   while (true) {
@@ -323,7 +325,7 @@ __device__ __forceinline__ u32 lookback_window(const u32* status, u32 tile, u32 
     excl += sum;
     if (found) return bad ? 0u : excl;
     if (stop < W) {
-      const u32 w = wait_status(status + (u64)(k - stop) * radix + d, err);
+      const u32 w = wait_status(status + (u64)(k - stop) * radix + d, err, limit_ns);
       const u32 f = w & 0xC0000000u;
       if (f == ST_ERR) {
         bad = true;
@@ -730,7 +732,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     }
     sexcl[d] = run;
     sbase[d] = run;
-    if (!a.tile_base) st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | run);
+    if (!a.tile_base && tile != a.withhold_tile) st_relaxed(st + d, (first_tile ? ST_INC : ST_AGG) | run);
   }
   __syncthreads();
   block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
@@ -746,8 +748,8 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     u32 excl = 0;
     bool bad = false;
     if (!first_tile) {
-      excl = lookback_window<WIN>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, bad);
-      st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
+      excl = lookback_window<WIN>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, a.spin_ns, bad);
+      if (tile != a.withhold_tile) st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
     }
     if (bad) sflag[1] = 1u;
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
@@ -1495,8 +1497,25 @@ __global__ void k_fill_keys(K* out, u64 n) {
 struct Tuning {
   int max_digit_bits = 8;
   int two_phase = 1;  // later radix passes: counts + scan, no look-back
+  int spin_limit_us = (int)(kSpinLimitNs / 1000);
 };
 extern thread_local Tuning g_tuning;
+
+// Thread-local failure injection (jfx_set_fault).
+struct Fault {
+  int withhold_tile = 0;
+  int learned_fallback = 0;
+  int fail_workspace = 0;
+};
+extern thread_local Fault g_fault;
+
+// The workspace check of every entry point (fail_workspace forces a failure).
+inline int check_workspace(const Arena& ar, const void* workspace, size_t bytes) {
+  if (ar.overflow || !workspace || g_fault.fail_workspace)
+    return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed%s", bytes, ar.off,
+                g_fault.fail_workspace ? " (failure injected by jfx_set_fault)" : "");
+  return JFX_OK;
+}
 
 // Pinned host scratch for the few words an entry point reads back.
 struct HostScratch {
@@ -1659,6 +1678,8 @@ inline u64 max_status_words(u64 n) {
 
 inline int launch_tile_scan(int radix, const u32* counts, u64 tiles, const u32* bin_base, u32* base, u32* totals,
                             u32* starts, u32* done, cudaStream_t s, u32 rot = 0) {
+  static SmemAttr attr;
+  if (tiles >= 32768) JFX_TRY(ensure_smem(attr, k_tile_scan<1024>, tile_scan_smem<1024>()));
   if (tiles >= 32768)
     k_tile_scan<1024><<<radix, 1024, tile_scan_smem<1024>(), s>>>(counts, tiles, bin_base, base, totals, starts, done,
                                                                 rot), note_launch();
@@ -1693,15 +1714,14 @@ inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles 
   using L = PassLayout<K, RB, NW>;
   if (TP && (!a.tile_base || a.digit_mode != DIG_BITS || a.segmented))
     return fail(JFX_ERR_ARG, "two-phase pass without tile bases or with non-bit digits");
-  static bool attr_set = false;  // per instantiation
-  if (!attr_set) {
-    JFX_CUDA(cudaFuncSetAttribute(k_onesweep<K, RB, FM, NW, TP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)L::SMEM));
-    attr_set = true;
-  }
+  static SmemAttr attr;  // per instantiation
+  JFX_TRY(ensure_smem(attr, k_onesweep<K, RB, FM, NW, TP>, L::SMEM));
   int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
+  PassArgs pa = a;
+  pa.spin_ns = (u64)g_tuning.spin_limit_us * 1000ull;
+  pa.withhold_tile = g_fault.withhold_tile > 0 ? (u32)g_fault.withhold_tile : 0u;
   const long t = timing_begin(s);
-  k_onesweep<K, RB, FM, NW, TP><<<tiles, L::THREADS, L::SMEM, s>>>(a), note_launch();
+  k_onesweep<K, RB, FM, NW, TP><<<tiles, L::THREADS, L::SMEM, s>>>(pa), note_launch();
   if (t >= 0) {
     // algorithmic bytes: the first pass reads the key columns and writes
     // key + row id; later passes read and write key + row id
@@ -1813,15 +1833,10 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
   {
     int grid = (int)std::min<u64>((n + 1023) / 1024, (u64)device_sm_count() * 4);
     size_t smem = (size_t)npass * RADIX * sizeof(u32);
-    static bool attr = false;
-    if (!attr) {
-      JFX_CUDA(cudaFuncSetAttribute(k_hist<K, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * 2048 * 4));
-      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u64, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
-      JFX_CUDA(cudaFuncSetAttribute(k_hist_int<K, u32, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 9 * 2048 * 4));
-      JFX_CUDA(cudaFuncSetAttribute(k_tile_scan<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)tile_scan_smem<1024>()));
-      attr = true;
-    }
+    static SmemAttr a_hist, a_hist64, a_hist32;
+    JFX_TRY(ensure_smem(a_hist, k_hist<K, RB>, 8 * 2048 * 4));
+    JFX_TRY(ensure_smem(a_hist64, k_hist_int<K, u64, RB>, 9 * 2048 * 4));
+    JFX_TRY(ensure_smem(a_hist32, k_hist_int<K, u32, RB>, 9 * 2048 * 4));
     if (int_key) {
       HistIntArgs hi;
       memset(&hi, 0, sizeof hi);

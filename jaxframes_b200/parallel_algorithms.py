@@ -344,7 +344,11 @@ def _run_groupby(keys, values: dict, agg_funcs: dict, multi: bool):
         check(L.jfx_groupby(karr, len(cols), n, 1 if multi else 0, varr, len(agg_cols), uptrs, ctypes.byref(G),
                             ws.data_ptr(), ws.numel(), _stream()))
     g = G.value
-    return [u[:g] for u in uniq], {c: outputs[c][:g] for c in agg_funcs}
+    # the kernels write into n-row buffers (G is known only after they ran);
+    # when the groups are much fewer than the rows, copy the G rows out so the
+    # caller does not keep the n-row storage alive
+    fit = (lambda t: t[:g].clone()) if 2 * g < n else (lambda t: t[:g])
+    return [fit(u) for u in uniq], {c: fit(outputs[c]) for c in agg_funcs}
 
 
 class SortBasedGroupBy:

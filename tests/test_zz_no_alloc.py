@@ -78,7 +78,11 @@ def _cases():
     k2[2::89] = 0.0
     # small int32 call after the large ones (stale data in the array)
     k3 = rng.integers(-1000, 1000, 1003, dtype=np.int64).astype(np.int32)
-    return [(k1, True), (k2, False), (k3, True)]
+    # descending integer keys (the whole order reversed, ties included)
+    k4 = rng.integers(-(1 << 50), 1 << 50, 200_003, dtype=np.int64)
+    k4[::3] = k4[11]
+    k5 = rng.integers(-50_000, 50_000, MAX_ROWS, dtype=np.int64).astype(np.int32)
+    return [(k1, True), (k2, False), (k3, True), (k4, False), (k5, False)]
 
 
 @pytest.mark.gpu
@@ -95,3 +99,21 @@ def test_static_sort_matches_workspace_sort_on_consecutive_calls():
             # bit patterns, so NaN and the sign of zero compare exactly
             np.testing.assert_array_equal(keys.view(np.uint8), want_keys.view(np.uint8))
         assert np.array_equal(np.sort(perm), np.arange(len(key_np)))  # a permutation
+
+
+@pytest.mark.gpu
+def test_static_sort_matches_the_oracle():
+    """One case straight against the oracle's restatement of
+    ParallelRadixSort.sort (parallel_algorithms.py:463-581)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from oracle import jfx_oracle as O
+    lib = _library()
+    rng = np.random.default_rng(72)
+    for ascending in (True, False):
+        key_np = rng.integers(-(1 << 33), 1 << 33, 250_007, dtype=np.int64)
+        key_np[::4] = key_np[5]
+        perm, keys = _run(lib, True, torch.from_numpy(key_np).cuda(), ascending)
+        want_keys, want_perm = O.radix_sort(key_np, np.arange(len(key_np)), ascending=ascending)
+        np.testing.assert_array_equal(perm, want_perm)
+        np.testing.assert_array_equal(keys, want_keys)
