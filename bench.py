@@ -47,6 +47,23 @@ def make_join_inputs(nl=NL, nr=NR, seed=43):
     return lk, lv, rk, rv
 
 
+def make_join_shard(rank, world, nl=NL, nr=NR):
+    """Rank ``rank``'s shard of the join scaled to ``world`` ranks (weak
+    scaling): ``nl`` left rows with keys uniform in [0, world * nr) and ``nr``
+    right rows holding the keys [rank * nr, (rank + 1) * nr) in random order,
+    so that the right keys of all ranks are one permutation of
+    0..world * nr - 1 and every left row matches exactly one right row.  With
+    world == 1 this is ``make_join_inputs``."""
+    if world == 1:
+        return make_join_inputs(nl, nr)
+    rng = np.random.default_rng(43 + 1000 * rank)
+    lk = rng.integers(0, world * nr, nl, dtype=np.int64)
+    lv = rng.standard_normal(nl, dtype=np.float32)
+    rk = (rng.permutation(nr) + rank * nr).astype(np.int64)
+    rv = rng.integers(-2**31, 2**31, nr, dtype=np.int64).astype(np.int32)
+    return lk, lv, rk, rv
+
+
 def c3_inputs(n=100_000_000, seed=44):
     """Multi-key groupby input: k1 truncated Zipf(s=1.1) over 1M ranks mapped
     through a permutation, k2 uniform in [0, 64), v1 N(0,1) float32, v2 uniform
@@ -220,6 +237,74 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- parity ---
+def check_join_parity(mk, out, lk, lv, rk, rv):
+    """The join's merged keys and payloads against the oracle's
+    ParallelSortMergeJoin.join (parallel_algorithms.py:938-1075), bit-exact."""
+    from oracle import jfx_oracle as O
+    t0 = time.perf_counter()
+    emk, eout, _, _ = O.sort_merge_join(lk, {"lv": lv}, rk, {"rv": rv}, "inner")
+    ok = mk.numel() == len(emk) and np.array_equal(mk.cpu().numpy(), emk)
+    for c, e in eout.items():
+        g = out[c].cpu().numpy()
+        ok = ok and g.dtype == e.dtype and np.array_equal(g.view(np.uint8), e.view(np.uint8))
+    return {"ok": bool(ok), "against": "oracle, bit-exact", "rows": int(len(emk)),
+            "check_s": round(time.perf_counter() - t0, 1)}
+
+
+def stable_argsort_ok(keys, perm):
+    """On the device: ``perm`` is the stable ascending argsort of uint64
+    ``keys`` -- a permutation, keys non-decreasing along it, and equal keys in
+    ascending row order.  These three properties determine the stable argsort
+    uniquely, so this is the same check as comparing with
+    ``np.argsort(kind="stable")``."""
+    import torch
+    n = keys.numel()
+    p = perm.long()
+    if n == 0:
+        return True
+    if int(p.min()) < 0 or int(p.max()) >= n:
+        return False
+    seen = torch.zeros(n, dtype=torch.bool, device=keys.device)
+    seen[p] = True
+    if not bool(seen.all()):
+        return False
+    del seen
+    s = keys.view(torch.int64)[p] ^ torch.iinfo(torch.int64).min  # unsigned order as signed
+    ok = bool((s[1:] >= s[:-1]).all())
+    ties = s[1:] == s[:-1]
+    ok = ok and bool((p[1:] > p[:-1])[ties].all())
+    return ok
+
+
+def check_groupby_parity(k1, k2, v1, v2, got_keys, got):
+    """groupby_aggregate_multi_column (:662-731, :1212-1242) against the
+    oracle: keys, counts, min/max and integer sums bit-exact, float32 sums
+    within 2^-16 * sum(|x|) per group, means within that over the count."""
+    from oracle import jfx_oracle as O
+    t0 = time.perf_counter()
+    hv = {f"v1_{a}": v1 for a in ("sum", "mean", "min", "max", "count")}
+    hv.update({f"v2_{a}": v2 for a in ("sum", "mean", "min", "max", "count")})
+    aggs = {c: c.split("_")[1] for c in hv}
+    hv["abs_v1"] = np.abs(v1).astype(np.float64)
+    ek, eout = O.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], hv, dict(aggs, abs_v1="sum"))
+    ok = all(np.array_equal(got_keys[k], ek[k]) for k in ("k1", "k2"))
+    asum, cnt = eout["abs_v1"], eout["v1_count"]
+    for c in aggs:
+        g, e = got[c], eout[c]
+        if not ok or g.dtype != e.dtype or len(g) != len(e):
+            ok = False
+            break
+        if c == "v1_sum":
+            ok = bool((np.abs(g.astype(np.float64) - e) <= asum * 2.0 ** -16 + 1e-30).all())
+        elif c == "v1_mean":
+            ok = bool((np.abs(g.astype(np.float64) - e) <= asum / cnt * 2.0 ** -16 + 1e-30).all())
+        else:
+            ok = bool(np.array_equal(g, e))
+    return {"ok": bool(ok), "against": "oracle (float32 sums within 2^-16 sum|x|)", "groups": int(len(ek["k1"])),
+            "check_s": round(time.perf_counter() - t0, 1)}
+
+
 # ------------------------------------------------------------------- GPU ---
 def run_gpu(args):
     import torch
@@ -242,14 +327,22 @@ def run_gpu(args):
     import jaxframes_b200.parallel_algorithms as P
     L = _lib.load_library()
 
-    lk, lv, rk, rv = make_join_inputs()
+    lk, lv, rk, rv = make_join_shard(rank, world)
     dev = torch.device("cuda", local)
     d_lk, d_lv = torch.from_numpy(lk).to(dev), torch.from_numpy(lv).to(dev)
     d_rk, d_rv = torch.from_numpy(rk).to(dev), torch.from_numpy(rv).to(dev)
     joiner = P.ParallelSortMergeJoin()
 
+    def join(a, av, b, bv):
+        # one GPU: the join itself; several: both sides repartitioned by
+        # hash(key) % world over NCCL, then the local join on every rank
+        if world == 1:
+            return joiner.join(a, av, b, bv, "inner")
+        from jaxframes_b200.distributed import distributed_join
+        return distributed_join(a, av, b, bv, "inner")
+
     def step():
-        return joiner.join(d_lk, {"lv": d_lv}, d_rk, {"rv": d_rv}, "inner")
+        return join(d_lk, {"lv": d_lv}, d_rk, {"rv": d_rv})
 
     def barrier():
         if world > 1:
@@ -302,7 +395,11 @@ def run_gpu(args):
     outs_h = {}
 
     def e2e_step():
-        mk, out = joiner.join(h[0], {"lv": h[1]}, h[2], {"rv": h[3]}, "inner")
+        if world == 1:
+            mk, out = joiner.join(h[0], {"lv": h[1]}, h[2], {"rv": h[3]}, "inner")
+        else:
+            a, av, b, bv = (x.to(dev, non_blocking=True) for x in h)
+            mk, out = join(a, {"lv": av}, b, {"rv": bv})
         res = [mk, out["left_lv"], out["right_rv"]]
         nbytes = 0
         for i, t in enumerate(res):
@@ -346,9 +443,31 @@ def run_gpu(args):
     value = rows / (ms / 1000)
     model = join_model_bytes(NL, NR, m_rows)
 
+    # parity of the timed call's output against the oracle at full size
+    # (outside the timed region).  Several ranks: each rank checks its local
+    # join on the rows the exchange brought it (the exchange itself is
+    # checked with gloo ranks in the tests); the flags are AND-ed over ranks.
+    parity = None
+    if not args.no_check:
+        if world == 1:
+            parity = check_join_parity(mk, out, lk, lv, rk, rv)
+        else:
+            from jaxframes_b200.repartition import exchange_partitions
+            (xl,), xlv, _ = exchange_partitions([d_lk], {"lv": d_lv})
+            (xr,), xrv, _ = exchange_partitions([d_rk], {"rv": d_rv})
+            parity = check_join_parity(mk, out, xl.cpu().numpy(), xlv["lv"].cpu().numpy(), xr.cpu().numpy(),
+                                       xrv["rv"].cpu().numpy())
+            ok = torch.tensor([1 if parity["ok"] else 0], device=dev)
+            rows_all = torch.tensor([int(mk.numel())], device=dev)
+            dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+            dist.all_reduce(rows_all, op=dist.ReduceOp.SUM)
+            parity.update(ok=bool(ok.item()), against="oracle, bit-exact, per rank on its exchanged rows",
+                          rows=int(rows_all.item()), expected_rows=NL * world)
+            parity["ok"] = parity["ok"] and parity["rows"] == NL * world
+
     extra = {}
     if args.extra and rank == 0 and world == 1:
-        extra = run_extra(args, P, dev)
+        extra = run_extra(args, P, dev, hbm, check=not args.no_check)
 
     if rank == 0:
         cpu_v, reps = cpu_join_sample(NL // 10, NR // 10, seconds=args.cpu_seconds)
@@ -356,9 +475,11 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "left_rows": NL, "right_rows": NR, "output_rows": m_rows,
-                       "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "l2": "inputs 180 MB > 126 MB L2, no flush"},
+            "config": {"workload": WORKLOAD, "left_rows": NL * world, "right_rows": NR * world,
+                       "rows_per_rank": [NL, NR], "output_rows_rank0": m_rows,
+                       "parallelism": (f"hash-repartitioned over {world} ranks (NCCL all_to_all, then local join)"
+                                       if world > 1 else "single"),
+                       "l2": "inputs 180 MB per rank > 126 MB L2, no flush"},
             "model_gbs": model / (ms / 1000) / 1e9,
             "model_frac": model / (ms / 1000) / 1e9 / hbm,
             "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix pass)", "achieved": achieved,
@@ -369,6 +490,8 @@ def run_gpu(args):
             "e2e": {"value": (NL + NR) * world / (e2e_ms / 1000), "unit": "rows/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "gpu_launches": launches,
+            "parity_checked": bool(parity and parity["ok"]),
+            "parity": parity,
             "clocks": clocks,
             "cpu_baseline": {"value": cpu_v, "unit": "rows/s", "cores": 1, "kind": "port",
                              "sample": f"inner join {NL // 10} x {NR // 10} rows x {reps} reps, single-threaded "
@@ -449,19 +572,19 @@ def run_secondary(args):
           flush=True)
 
 
-def run_batch(args, dev):
-    """Batched hash partition (256 partitions) + groupby-sum over 2048 queries
-    with row counts floor(exp(uniform(ln 1e3, ln 4e6))) (about 1e9 rows),
-    int32 keys uniform in [0, min(rows // 4, 1e6)), float32 N(0, 1) values;
-    one CUDA-graph replay per step.  Inputs are generated on the device from a
-    seeded generator."""
+def c5_batch(dev, total_rows=0, nq=2048):
+    """The batched workload: 2048 queries with row counts
+    floor(exp(uniform(ln 1e3, ln 4e6))) (about 1e9 rows; scaled to about
+    ``total_rows`` when given), int32 keys uniform in [0, min(rows // 4, 1e6)),
+    float32 N(0, 1) values, hash partition to 256 partitions then groupby-sum.
+    Inputs are generated on the device from a seeded generator straight into a
+    ``BatchedGroupBy``'s buffers; returns it and the host row offsets."""
     import torch
     from jaxframes_b200.batch import BatchedGroupBy
-    nq = 2048
     rng = np.random.default_rng(46)
     rows = np.floor(np.exp(rng.uniform(np.log(1e3), np.log(4e6), nq))).astype(np.int64)
-    if args.n:  # scaled-down batch with the same shape of row counts
-        rows = np.maximum(1, np.floor(rows * (args.n / rows.sum()))).astype(np.int64)
+    if total_rows:  # scaled-down batch with the same shape of row counts
+        rows = np.maximum(1, np.floor(rows * (total_rows / rows.sum()))).astype(np.int64)
     off = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
     n = int(off[-1])
     b = BatchedGroupBy(n, nq, 256, 20, device=dev)
@@ -473,6 +596,48 @@ def run_batch(args, dev):
                                                   dtype=torch.int32)
     torch.randn(n, generator=g, device=dev, out=b.values[:n])
     b.query_offsets.copy_(torch.from_numpy(off))
+    return b, off
+
+
+def check_batch_queries(b, off, queries, num_partitions=256):
+    """Per-query parity of a batched run against the oracle: partition
+    offsets, partitioned keys and values and group keys and counts bit-exact,
+    sums within 2^-16 * sum(|x|) per group.  Returns the number of rows
+    checked; raises AssertionError on a mismatch."""
+    from oracle import jfx_oracle as O
+    rows = 0
+    for q in queries:
+        a, e = int(off[q]), int(off[q + 1])
+        k = b.keys[a:e].cpu().numpy()
+        v = b.values[a:e].cpu().numpy()
+        po, pk, pv, gk, gs, gc = (t.cpu().numpy() for t in b.query(q))
+        _, perm, eoffs = O.hash_partition([k], num_partitions)
+        assert np.array_equal(po, eoffs), f"query {q}: partition offsets"
+        assert np.array_equal(pk, k[perm]) and np.array_equal(pv, v[perm]), f"query {q}: partitioned rows"
+        ek, eo = O.groupby_aggregate(k, {"s": v, "c": v, "a": np.abs(v).astype(np.float64)},
+                                     {"s": "sum", "c": "count", "a": "sum"})
+        assert np.array_equal(gk, ek) and np.array_equal(gc, eo["c"]), f"query {q}: groups"
+        assert (np.abs(gs.astype(np.float64) - eo["s"]) <= eo["a"] * 2.0 ** -16 + 1e-30).all(), f"query {q}: sums"
+        rows += e - a
+    return rows
+
+
+def batch_check_queries(off, count=64, seed=47):
+    """A seeded subset of the queries that includes the largest one."""
+    nq = len(off) - 1
+    largest = int(np.argmax(np.diff(off)))
+    others = np.delete(np.arange(nq), largest)
+    pick = np.random.default_rng(seed).choice(others, size=min(count, nq) - 1, replace=False).tolist()
+    return sorted(pick + [largest])
+
+
+def run_batch(args, dev):
+    """Batched hash partition (256 partitions) + groupby-sum over 2048 queries
+    (``c5_batch``); one CUDA-graph replay per step."""
+    import torch
+    b, off = c5_batch(dev, args.n)
+    nq = len(off) - 1
+    n = int(off[-1])
     b.capture()
     for _ in range(args.warmup):
         b.replay()
@@ -492,13 +657,18 @@ def run_batch(args, dev):
                       "graph": "one CUDA graph replay per step"}), flush=True)
 
 
-def run_extra(args, P, dev):
-    """Secondary measurements on the other configs (not the headline)."""
+def run_extra(args, P, dev, hbm=6650.0, check=True):
+    """The other configurations, each timed on the device (CUDA events, inputs
+    resident, larger than L2 except the 1M-row groupby) and checked against
+    the oracle outside the timed region.  Model bytes follow the fixed
+    per-row byte model of each operator (sort, groupby, batch); ``frac`` is
+    model GB/s over the measured HBM copy bandwidth."""
     import torch
     out = {}
 
-    def timeit(fn, steps):
-        fn()
+    def timeit(fn, steps, warm=1):
+        for _ in range(warm):
+            fn()
         torch.cuda.synchronize()
         a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -508,29 +678,53 @@ def run_extra(args, P, dev):
         torch.cuda.synchronize()
         return a.elapsed_time(b2) / steps
 
+    def roof(model, ms):
+        gbs = model / (ms / 1e3) / 1e9
+        return {"bound": "hbm", "model_bytes": model, "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm}
+
+    from oracle import jfx_oracle as O
     try:
         rng = np.random.default_rng(42)
         n = 1_000_000
-        k = torch.from_numpy(rng.integers(0, 1000, n).astype(np.int32)).to(dev)
-        v = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+        kh = rng.integers(0, 1000, n).astype(np.int32)
+        vh = rng.standard_normal(n).astype(np.float32)
+        k, v = torch.from_numpy(kh).to(dev), torch.from_numpy(vh).to(dev)
         ms = timeit(lambda: P.groupby_aggregate(k, {"v": v, "c": v}, {"v": "sum", "c": "count"}), 5)
-        out["groupby_sum_1M"] = {"ms": ms, "rows_per_s": n / (ms / 1e3)}
+        res = {"ms": ms, "rows_per_s": n / (ms / 1e3), "roofline": roof(n * 24 + 1000 * 12, ms)}
+        if check:
+            uk, o = P.groupby_aggregate(k, {"v": v, "c": v}, {"v": "sum", "c": "count"})
+            ek, eo = O.groupby_aggregate(kh, {"v": vh, "c": vh, "a": np.abs(vh).astype(np.float64)},
+                                         {"v": "sum", "c": "count", "a": "sum"})
+            ok = (np.array_equal(uk.cpu().numpy(), ek) and np.array_equal(o["c"].cpu().numpy(), eo["c"])
+                  and bool((np.abs(o["v"].cpu().numpy().astype(np.float64) - eo["v"]) <= eo["a"] * 2.0 ** -16).all()))
+            res["parity_checked"] = bool(ok)
+        out["groupby_sum_1M"] = res
     except Exception as e:  # report, do not hide
         out["groupby_sum_1M"] = {"error": repr(e)}
     try:
-        k1, k2, v1, v2 = [torch.from_numpy(x).to(dev) for x in c3_inputs()]
+        hk1, hk2, hv1, hv2 = c3_inputs()
+        k1, k2, v1, v2 = [torch.from_numpy(x).to(dev) for x in (hk1, hk2, hv1, hv2)]
         vals = {f"v1_{a}": v1 for a in ("sum", "mean", "min", "max", "count")}
         vals.update({f"v2_{a}": v2 for a in ("sum", "mean", "min", "max", "count")})
         aggs = {c: c.split("_")[1] for c in vals}
-        res = {}
-        ms = timeit(lambda: res.setdefault("r", P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)),
-                    3)
-        g = int(P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)[0]["k1"].numel())
+        ms = timeit(lambda: P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs), 3)
+        uk, o = P.groupby_aggregate_multi_column([k1, k2], ["k1", "k2"], vals, aggs)
+        g = int(uk["k1"].numel())
         n = k1.numel()
+        # SORT(N, K=4, Kraw=8) with P = ceil(26 / 11) = 3 passes, the value
+        # reads, and 60 bytes of key and aggregate outputs per group
         model = n * (8 + 8 + 2 * 2 * 8) + n * (4 + 4 + 4 + 8) + g * 60
-        out["groupby_multikey_100M"] = {"ms": ms, "rows_per_s": n / (ms / 1e3), "groups": g,
-                                        "model_gbs": model / (ms / 1e3) / 1e9}
-        del k1, k2, v1, v2, vals
+        res = {"ms": ms, "rows_per_s": n / (ms / 1e3), "groups": g, "model_gbs": model / (ms / 1e3) / 1e9,
+               "roofline": roof(model, ms)}
+        got_keys = {kk: t.cpu().numpy() for kk, t in uk.items()}
+        got = {c: t.cpu().numpy() for c, t in o.items()}
+        del k1, k2, v1, v2, vals, uk, o
+        torch.cuda.empty_cache()
+        if check:
+            res["parity"] = check_groupby_parity(hk1, hk2, hv1, hv2, got_keys, got)
+            res["parity_checked"] = res["parity"]["ok"]
+        out["groupby_multikey_100M"] = res
+        del hk1, hk2, hv1, hv2, got, got_keys
     except Exception as e:
         out["groupby_multikey_100M"] = {"error": repr(e)}
     try:
@@ -540,11 +734,63 @@ def run_extra(args, P, dev):
         s = P.ParallelRadixSort()
         ms = timeit(lambda: s.argsort(keys), 2)
         model = n * (8 + 12 + 5 * 24)
-        out["sort_u64_256M_uniform"] = {"ms": ms, "keys_per_s": n / (ms / 1e3), "model_gbs": model / (ms / 1e3) / 1e9}
+        res = {"ms": ms, "keys_per_s": n / (ms / 1e3), "model_gbs": model / (ms / 1e3) / 1e9,
+               "roofline": roof(model, ms)}
+        if check:
+            res["parity_checked"] = stable_argsort_ok(keys, s.argsort(keys))
+        out["sort_u64_256M_uniform"] = res
         del keys
+        torch.cuda.empty_cache()
     except Exception as e:
         out["sort_u64_256M_uniform"] = {"error": repr(e)}
-    torch.cuda.empty_cache()
+    try:
+        keys = torch.from_numpy(c4_keys()).to(dev)
+        n = keys.numel()
+        model = n * (8 + 12 + 5 * 24)  # the plain sort's model bytes, the denominator of both forms
+        res = {"rows": n}
+        for mode in ("plain", "auto"):
+            ms = timeit(lambda: P.learned_sort(keys, mode=mode), 3)
+            res["learned" if mode == "auto" else "plain"] = {"ms": ms, "model_gbs": model / (ms / 1e3) / 1e9}
+        sk_p, perm_p, _ = P.learned_sort(keys, mode="plain")
+        del sk_p
+        sk_l, perm_l, used = P.learned_sort(keys, mode="auto")
+        res["learned_used"] = used
+        res["identical_perm"] = bool(torch.equal(perm_p, perm_l))
+        del sk_l, perm_l
+        res["speedup"] = res["plain"]["ms"] / res["learned"]["ms"]
+        res["roofline"] = roof(model, res["learned"]["ms"])
+        if check:
+            res["parity_checked"] = res["identical_perm"] and stable_argsort_ok(keys, perm_p)
+        out["learned_c4_256M"] = res
+        del keys, perm_p
+        torch.cuda.empty_cache()
+    except Exception as e:
+        out["learned_c4_256M"] = {"error": repr(e)}
+    try:
+        b, off = c5_batch(dev)
+        nq, n = len(off) - 1, int(off[-1])
+        b.capture()
+        ms = timeit(b.replay, 3, warm=2)
+        b.status()
+        groups = int(b.group_offsets[nq].item())
+        model = 56 * n + 8 * groups  # partition 16 + sort 28 + groupby 12 bytes per row, 8 per group
+        res = {"ms": ms, "queries": nq, "rows": n, "groups": groups, "rows_per_s": n / (ms / 1e3),
+               "model_gbs": model / (ms / 1e3) / 1e9, "roofline": roof(model, ms),
+               "graph": "one CUDA graph replay per step"}
+        if check:
+            qs = batch_check_queries(off)
+            try:
+                rows = check_batch_queries(b, off, qs)
+                res["parity_checked"] = True
+                res["parity"] = {"ok": True, "queries": len(qs), "rows": rows, "includes_largest": True}
+            except AssertionError as e:
+                res["parity_checked"] = False
+                res["parity"] = {"ok": False, "error": str(e)}
+        out["batch_c5_2048q"] = res
+        del b
+        torch.cuda.empty_cache()
+    except Exception as e:
+        out["batch_c5_2048q"] = {"error": repr(e)}
     return out
 
 
@@ -560,6 +806,7 @@ def main():
                     help="join = the headline; the others time one secondary config alone")
     ap.add_argument("--n", type=int, default=0, help="rows for --workload groupby/sort (0 = config size)")
     ap.add_argument("--profile", action="store_true", help="timed steps only (no e2e, CPU leg or extras)")
+    ap.add_argument("--no-check", action="store_true", help="skip the parity checks against the oracle")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -220,14 +220,17 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
  * reference; its output is exactly the plain radix sort's: sorted keys and
  * the stable int32 permutation).  A 1% strided sample, sorted by the plain
  * radix sort, trains a two-level piecewise-linear model (root line plus 4096
- * leaf lines, least squares); radix passes over the model's predicted
- * position replace the key-digit passes, and runs of equal prediction are
- * sorted in a fix-up.  mode 0: learned, with the plain sort as fallback when
- * the model fails its monotonicity check or a run overflows the fix-up;
- * mode 1: plain radix sort only.  *learned_used (nullable) is 1 when the
- * learned path produced the result, 0 when the plain sort was asked for or
- * the input is small, and -1 / -2 / -3 when the learned path fell back
- * (model check failed / a run of equal prediction too long / run list full). */
+ * leaf lines, least squares) of each key's position.  The predicted
+ * position's top bits name a bucket of about 2048 rows; two stable radix
+ * passes over the bucket id move (key, row id) into bucket order, and each
+ * bucket is then sorted by key inside one CTA (a bucket too large for shared
+ * memory by one CTA in global memory, or above 2^20 rows by the plain radix
+ * sort).  mode 0: learned, with the plain sort as fallback when the model
+ * fails its monotonicity check or more than 4096 buckets are too large for
+ * shared memory; mode 1: plain radix sort only.  *learned_used (nullable) is
+ * 1 when the learned path produced the result, 0 when the plain sort was
+ * asked for or the input is small, and -1 / -3 when the learned path fell
+ * back (model check failed / large-bucket list full). */
 int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out, int32_t* perm_out,
                      int mode, int32_t* learned_used, void* workspace, size_t workspace_bytes,
                      void* stream);
@@ -284,9 +287,9 @@ int jfx_get_tuning(jfx_tuning* t);
  *                     that ticket never publishes its counts, so the later
  *                     tiles' bounded waits run out and the call returns
  *                     JFX_ERR_TIMEOUT (give a short spin_limit_us);
- *   learned_fallback: -1 / -2 / -3: jfx_learned_sort takes that fallback (model
- *                     check failed / run too long / run list full) as if its
- *                     own check had found it; the output is the plain sort's;
+ *   learned_fallback: -1 / -3: jfx_learned_sort takes that fallback (model
+ *                     check failed / large-bucket list full) as if its own
+ *                     check had found it; the output is the plain sort's;
  *   fail_workspace:   1: every entry point that takes a workspace reports it
  *                     as too small (JFX_ERR_ALLOC) before launching anything. */
 typedef struct {

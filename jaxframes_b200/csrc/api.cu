@@ -208,8 +208,8 @@ static int launch_join_count(const void* A, u64 na, const void* B, u64 nb, u32* 
 
 // ---------------------------------------------------------------- learned ---
 struct LearnedBuffers {
-  u32* pos;   // predicted position of each key, in row order
-  u32* spos;  // predicted position of each key, in sorted order
+  u32* pos;   // bucket of each key (predicted position >> kBucketShift), in row order
+  u32* spos;  // the buckets in sorted order
   u64* sample;
   u64* ssorted;
   u32* sperm;
@@ -219,9 +219,13 @@ struct LearnedBuffers {
   u32* first;
   u32* last;
   double* fit;
-  u32* flags;  // [0] ok
-  FixLists fix;
-  u64 s, tiles;
+  u32* flags;   // [0] model check passed
+  u32* starts;  // [buckets + 1]
+  u32* large;   // [kBucketLargeMax][2]
+  u32* bcounts; // [0] large buckets
+  u64* tkeys;   // scratch of the large-bucket sorts
+  u32* tids;
+  u64 s, nb;
 };
 static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBuffers& l) {
   take_common(ar, c);
@@ -239,17 +243,12 @@ static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBu
   l.last = ar.take<u32>(kLeaves);
   l.fit = ar.take<double>(2 * kLeaves);
   l.flags = ar.take<u32>(8);
-  l.tiles = (n + kFindTile - 1) / kFindTile;
-  l.fix.cap_small = (u32)(n / 8 + 64);
-  l.fix.cap_medium = (u32)(n / 512 + 64);
-  l.fix.cap_long = (u32)(n / kFixMaxRun + 64);
-  l.fix.small = ar.take<u32>(2 * (u64)l.fix.cap_small);
-  l.fix.medium = ar.take<u32>(2 * (u64)l.fix.cap_medium);
-  l.fix.lng = ar.take<u32>(2 * (u64)l.fix.cap_long);
-  l.fix.counts = ar.take<u32>(8);
-  l.fix.last_start = ar.take<u32>(l.tiles + 1);
-  l.fix.scanned_to = ar.take<u32>(l.tiles + 1);
-  l.fix.carried_inv = ar.take<u32>(l.tiles + 1);
+  l.nb = ((4 * n) >> kBucketShift) + 1;  // positions lie in [0, 4n)
+  l.starts = ar.take<u32>(l.nb + 1);
+  l.large = ar.take<u32>(2 * kBucketLargeMax);
+  l.bcounts = ar.take<u32>(8);
+  l.tkeys = ar.take<u64>(n ? n : 1);
+  l.tids = ar.take<u32>(n ? n : 1);
 }
 
 // Plain radix sort of raw uint64 keys: sorted keys and row ids.
@@ -274,6 +273,32 @@ static int plain_sort_u64(const u64* keys, u64 n, u64* sorted_out, u32* perm_out
   }
   JFX_TRY(radix_sort(rq, n, b, c.err, s));
   if (kp.total_bits == 0) JFX_CUDA(cudaMemcpyAsync(sorted_out, keys, n * 8, cudaMemcpyDeviceToDevice, s));
+  return JFX_OK;
+}
+
+// Stable sort of the rows [0, m) of (keys, ids) by key (one large bucket of
+// the learned sort): the plain radix sort over the rows' key range, the ids
+// carried as the payload, through the scratch arrays and back.
+static int sort_rows_u64(u64* keys, u32* ids, u64 m, u64* tkeys, u32* tids, SortBuffers& b, Common& c,
+                         cudaStream_t s) {
+  jfx_column col{keys, JFX_U64, 0u};
+  KeyPlan kp;
+  JFX_TRY(build_pack(&col, 1, 0u, false, kp.pack));
+  JFX_TRY(plan_keys(kp, m, c.mm, s));
+  if (kp.total_bits == 0) return JFX_OK;  // one key: the rows are in row order already
+  RadixRequest rq;
+  rq.pack = kp.pack;
+  rq.total_bits = kp.total_bits;
+  rq.key64 = kp.total_bits > 32;
+  rq.nwords = 1;
+  rq.pfirst[0] = PayloadSrc{(const unsigned char*)ids, 4u, 0u};
+  rq.vout_final[0] = tids;
+  rq.raw_out = tkeys;
+  rq.raw_dtype = JFX_U64;
+  rq.raw_tmin = kp.pack.c[0].tmin;
+  JFX_TRY(radix_sort(rq, m, b, c.err, s));
+  JFX_CUDA(cudaMemcpyAsync(keys, tkeys, m * 8, cudaMemcpyDeviceToDevice, s));
+  JFX_CUDA(cudaMemcpyAsync(ids, tids, m * 4, cudaMemcpyDeviceToDevice, s));
   return JFX_OK;
 }
 
@@ -436,8 +461,8 @@ int jfx_set_fault(const jfx_fault* f) {
     return JFX_OK;
   }
   if (f->withhold_tile < 0) return fail(JFX_ERR_ARG, "withhold_tile must be >= 0, got %d", f->withhold_tile);
-  if (f->learned_fallback != 0 && f->learned_fallback != -1 && f->learned_fallback != -2 && f->learned_fallback != -3)
-    return fail(JFX_ERR_ARG, "learned_fallback must be 0, -1, -2 or -3, got %d", f->learned_fallback);
+  if (f->learned_fallback != 0 && f->learned_fallback != -1 && f->learned_fallback != -3)
+    return fail(JFX_ERR_ARG, "learned_fallback must be 0, -1 or -3, got %d", f->learned_fallback);
   if (f->fail_workspace != 0 && f->fail_workspace != 1)
     return fail(JFX_ERR_ARG, "fail_workspace must be 0 or 1, got %d", f->fail_workspace);
   g_fault.withhold_tile = f->withhold_tile;
@@ -1378,25 +1403,23 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   const u64 npos = 4 * N;
   k_leaf_finalize<<<1, 1024, 0, s>>>(l.ssorted, l.s, npos, l.first, l.last, l.fit, l.leaves, l.flags), note_launch();
   JFX_CUDA(cudaGetLastError());
-  // 3. radix passes over the predicted position: the first pass evaluates the
-  // model once per key and sorts by the position, carrying the key (two
-  // words) and the row id; the last pass writes the key as one u64
+  // 3. bucket of every key (the predicted position's top bits), then a
+  // plain stable radix sort of that uint32 column carrying the key's two
+  // words and the row id: rows in bucket order, row order inside a bucket
   {
-    // positions once (row order), then a plain sort of that uint32 column:
-    // its histogram kernel counts the first pass's tiles, so every pass runs
-    // in two phases with the lean integer-key first pass
-    k_model_positions<<<grid_for(N, 256), 256, 0, s>>>(keys, N, l.model, l.pos), note_launch();
+    k_model_positions<<<grid_for(N, 256), 256, 0, s>>>(keys, N, l.model, kBucketShift, l.pos), note_launch();
     JFX_CUDA(cudaGetLastError());
     jfx_column col{l.pos, JFX_U32, 0u};
     RadixRequest rq;
     JFX_TRY(build_pack(&col, 1, 0u, false, rq.pack));
-    rq.total_bits = std::max(1, bit_length(npos - 1));
+    rq.total_bits = std::max(1, bit_length(l.nb - 1));
     rq.pack.c[0].tmin = 0;
     rq.pack.c[0].bits = rq.total_bits;
     rq.pack.c[0].shift = 0;
     rq.key_mode = KEY_PACK;
     rq.digit_mode = DIG_BITS;
     rq.key64 = false;
+    rq.max_digit_bits = 9;  // 17 bucket bits at 2^28 rows: two passes of 9 + 8 bits
     rq.nwords = 3;
     rq.pfirst[0] = PayloadSrc{(const unsigned char*)keys, 8u, 0u};
     rq.pfirst[1] = PayloadSrc{(const unsigned char*)keys, 8u, 4u};
@@ -1406,38 +1429,68 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     rq.keys_out = l.spos;
     JFX_TRY(radix_sort(rq, N, b, c.err, s));
   }
-  // 4. fix-up of runs of equal predicted position
-  JFX_CUDA(cudaMemsetAsync(l.fix.counts, 0, 8 * sizeof(u32), s));
-  k_fix_find<<<(unsigned)l.tiles, kFindThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.spos, N, l.fix), note_launch();
-  k_fix_check<<<grid_for(l.tiles, 256), 256, 0, s>>>(l.tiles, l.fix), note_launch();
-  k_fix_small<<<device_sm_count() * 8, 256, 0, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
+  // 4. sort inside every bucket
+  JFX_CUDA(cudaMemsetAsync(l.bcounts, 0, 8 * sizeof(u32), s));
+  k_bucket_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(l.spos, N, (u32)l.nb, l.starts), note_launch();
   {
     static SmemAttr attr;
-    JFX_TRY(ensure_smem(attr, k_fix_medium, kFixMediumSmem));
+    JFX_TRY(ensure_smem(attr, k_bucket_sort, kBucketSmem));
+    BucketArgs ba;
+    ba.keys = sorted_keys_out;
+    ba.ids = (u32*)perm_out;
+    ba.starts = l.starts;
+    ba.nb = (u32)l.nb;
+    ba.large = l.large;
+    ba.counts = l.bcounts;
+    const int grid = (int)std::min<u64>(l.nb, (u64)device_sm_count() * 8);
+    k_bucket_sort<<<grid, kBucketThreads, kBucketSmem, s>>>(ba), note_launch();
+    // buckets of more rows than one CTA holds in shared memory (their count
+    // is read on the device: no synchronisation here)
+    LargeArgs la;
+    la.keys = sorted_keys_out;
+    la.ids = (u32*)perm_out;
+    la.tkeys = l.tkeys;
+    la.tids = l.tids;
+    la.large = l.large;
+    la.counts = l.bcounts;
+    k_bucket_sort_large<<<device_sm_count() * 2, kBucketThreads, 0, s>>>(la), note_launch();
   }
-  k_fix_medium<<<device_sm_count(), kFixMedThreads, kFixMediumSmem, s>>>(sorted_keys_out, (u32*)perm_out, l.fix), note_launch();
-  // long runs: the sort's ping-pong buffers are free now and serve as scratch
-  k_fix_long<<<device_sm_count(), kFixMedThreads, 0, s>>>(sorted_keys_out, (u32*)perm_out, (u64*)b.keys[0], b.vals[0][0], l.fix), note_launch();
   JFX_CUDA(cudaGetLastError());
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host + 1, l.flags, sizeof(u32), cudaMemcpyDeviceToHost, s));
-  JFX_CUDA(cudaMemcpyAsync(host + 2, l.fix.counts, 4 * sizeof(u32), cudaMemcpyDeviceToHost, s));
+  JFX_CUDA(cudaMemcpyAsync(host + 2, l.bcounts, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaStreamSynchronize(s));
   JFX_TRY(check_err_word((u32)host[0]));
   const u32 ok = (u32)host[1];
-  const u32* cnts = (const u32*)(host + 2);
-  if (!ok || cnts[2] || g_fault.learned_fallback) {
-    // model not monotone, or a run the fix-up cannot take: plain radix sort.
-    // *learned_used reports why: -1 model check, -2 run too long, -3 list full
-    // (or the fallback jfx_set_fault asked for)
-    const int why = g_fault.learned_fallback ? g_fault.learned_fallback
-                    : !ok                   ? -1
-                    : (cnts[2] & FIX_LONG_RUN) ? -2
-                                              : -3;
+  const u32 nlarge = (u32)host[2];
+  if (!ok || nlarge > kBucketLargeMax || g_fault.learned_fallback) {
+    // model not monotone, or more large buckets than listed: plain radix
+    // sort.  *learned_used reports why: -1 model check, -3 list full (or the
+    // fallback jfx_set_fault asked for)
+    const int why = g_fault.learned_fallback ? g_fault.learned_fallback : !ok ? -1 : -3;
     JFX_TRY(plain_sort_u64(keys, N, sorted_keys_out, (u32*)perm_out, b, c, s));
     JFX_TRY(read_back(c.err, sizeof(u32), host, s));
     if (learned_used) *learned_used = why;
     return check_err_word((u32)host[0]);
+  }
+  if (nlarge) {
+    // listed buckets of more than kLargeCtaMax rows (many rows of a few keys
+    // the model puts in one bucket): the multi-CTA stable radix sort of
+    // their rows, one call each
+    std::vector<u32> spans(2 * (size_t)nlarge);
+    JFX_CUDA(cudaMemcpyAsync(spans.data(), l.large, spans.size() * sizeof(u32), cudaMemcpyDeviceToHost, s));
+    JFX_CUDA(cudaStreamSynchronize(s));
+    bool any = false;
+    for (u32 r = 0; r < nlarge; ++r) {
+      const u64 b0 = spans[2 * r], b1 = spans[2 * r + 1];
+      if (b1 - b0 <= kLargeCtaMax) continue;
+      JFX_TRY(sort_rows_u64(sorted_keys_out + b0, (u32*)perm_out + b0, b1 - b0, l.tkeys, l.tids, b, c, s));
+      any = true;
+    }
+    if (any) {
+      JFX_TRY(read_back(c.err, sizeof(u32), host, s));
+      JFX_TRY(check_err_word((u32)host[0]));
+    }
   }
   if (learned_used) *learned_used = 1;
   return JFX_OK;

@@ -9,16 +9,17 @@
 //    (radix.cuh: model_pos).  Slopes are forced >= 0 and leaf ranges are
 //    disjoint and increasing, so the predicted position is monotone in x;
 //    k_leaf_finalize verifies it.
-// 3. Stable radix passes over the bits of the predicted position (not of x)
-//    move (key, row id) pairs: ceil(log2(n) / 11) passes instead of
-//    ceil(63 / 11).
-// 4. The position is monotone, so keys with different positions are already
-//    in order and only runs of equal position can hold inversions.
-//    k_fix_find lists the runs that hold one; k_fix_small (a warp per run)
-//    and k_fix_medium (a block radix sort per run) sort them by key -- equal
-//    keys keep row order because every pass is stable.  A run longer than
-//    kFixMaxRun, a full run list or a failed check make the caller fall back
-//    to the plain radix sort.  Either way the output equals the plain sort's.
+// 3. The predicted position's top bits name a bucket of about 2048 rows.
+//    Two stable radix passes over the bucket id (not over the key's 64 bits)
+//    move (key, row id) pairs into bucket order, row order inside a bucket.
+// 4. The model is monotone, so every key of a bucket is <= every key of the
+//    next bucket and only the order inside a bucket is left: k_bucket_sort
+//    sorts each bucket of up to kBucketCap rows in shared memory by the key
+//    bits that vary inside it (stable, so equal keys keep row order); a
+//    bucket of more rows is listed, and the host sorts its rows with the
+//    plain stable radix sort.  A failed model check makes the caller fall
+//    back to the plain radix sort.  Either way the output equals the plain
+//    sort's.
 #pragma once
 
 #include "radix.cuh"
@@ -175,8 +176,9 @@ __global__ void __launch_bounds__(1024) k_leaf_finalize(const u64* sx, u64 s, u6
   }
 }
 
-// Predicted position of every key, in row order.
-__global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n, const ModelRef* mp, u32* pos) {
+// Predicted position of every key >> shift (its bucket), in row order.
+__global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n, const ModelRef* mp, int shift,
+                                                         u32* pos) {
   const ModelRef m = *mp;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   constexpr int U = 4;
@@ -186,476 +188,286 @@ __global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n,
     for (int u = 0; u < U; ++u) k[u] = i0 + u * stride < n ? __ldg(keys + i0 + u * stride) : 0ull;
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (i0 + u * stride < n) pos[i0 + u * stride] = model_pos(m, k[u]);
+      if (i0 + u * stride < n) pos[i0 + u * stride] = model_pos(m, k[u]) >> shift;
   }
 }
 
-// ------------------------------------------------------------------ fix-up ---
-constexpr int kFindTile = 2048, kFindThreads = 256;
-constexpr int kFixMaxRun = 6144;   // longest run the shared-memory block sort takes
-constexpr u32 kFixLongMax = 1u << 20;  // longest run the global-memory sort takes
-constexpr int kFixSmall = 32;      // runs up to this length: one warp
+// ------------------------------------------------------------- buckets ---
+constexpr int kBucketShift = 13;  // positions in [0, 4n): 8192 positions, about 2048 rows, per bucket
+constexpr int kBucketThreads = 256, kBucketIPT = 16;
+constexpr u32 kBucketCap = kBucketThreads * kBucketIPT;  // rows one CTA sorts in shared memory
+constexpr u32 kBucketLargeMax = 4096;                     // large buckets listed per call
+constexpr u32 kLargeCtaMax = 1u << 20;  // larger buckets: the multi-CTA radix sort, one call each
 
-struct FixLists {
-  u32* small;       // [cap_small][2] (start, end)
-  u32* medium;      // [cap_medium][2]
-  u32* lng;         // [cap_long][2]
-  u32* counts;      // [0] small, [1] medium, [2] overflow flag, [3] long
-  u32* last_start;  // [tiles] last run start in the tile, or ~0
-  u32* carried_inv; // [tiles] first inversion of the run carried into the tile, or ~0
-  u32* scanned_to;  // [tiles] position up to which the tile's last run was scanned
-  u32 cap_small, cap_medium, cap_long;
+// starts[c] = first row of bucket c in the bucket-sorted ids sb[0..n), for
+// c in [0, nb]; an empty bucket starts where the next non-empty one does.
+__global__ void k_bucket_starts(const u32* sb, u64 n, u32 nb, u32* starts) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (u64)gridDim.x * blockDim.x) {
+    const u32 lo = i == 0 ? 0u : sb[i - 1] + 1u;  // buckets that start at row i
+    const u32 hi = i == n ? nb : sb[i];
+    for (u32 c = lo; c <= hi && c <= nb; ++c) starts[c] = (u32)i;
+  }
+}
+
+struct BucketArgs {
+  u64* keys;           // in/out: rows in bucket order (row order inside a bucket)
+  u32* ids;            // in/out: their row ids
+  const u32* starts;   // [nb + 1]
+  u32 nb;
+  u32* large;          // [kBucketLargeMax][2] buckets of more than kBucketCap rows: (start, end)
+  u32* counts;         // [0] large buckets found
 };
 
-// counts[2] bits: why the fix-up cannot finish (the caller falls back)
-enum : u32 { FIX_LONG_RUN = 1u, FIX_SMALL_FULL = 2u, FIX_MEDIUM_FULL = 4u };
-
-__device__ __forceinline__ void fix_record(const FixLists& L, u64 s, u64 e) {
-  const u64 len = e - s;
-  if (len > (u64)kFixLongMax) {
-    atomicOr(&L.counts[2], FIX_LONG_RUN);
-    return;
+// Min and max key of rows [s, e), by the whole CTA (red: 2 * warps words).
+__device__ __forceinline__ void block_minmax(const u64* keys, u32 s, u32 e, u64* red, u64& mn, u64& mx) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  mn = ~0ull;
+  mx = 0ull;
+  for (u32 j = s + threadIdx.x; j < e; j += blockDim.x) {
+    const u64 k = keys[j];
+    mn = k < mn ? k : mn;
+    mx = k > mx ? k : mx;
   }
-  if (len > (u64)kFixMaxRun) {
-    const u32 r = atomicAdd(&L.counts[3], 1u);
-    if (r >= L.cap_long) { atomicOr(&L.counts[2], FIX_MEDIUM_FULL); return; }
-    L.lng[2 * r] = (u32)s;
-    L.lng[2 * r + 1] = (u32)e;
-    return;
-  }
-  if (len <= (u64)kFixSmall) {
-    const u32 r = atomicAdd(&L.counts[0], 1u);
-    if (r >= L.cap_small) { atomicOr(&L.counts[2], FIX_SMALL_FULL); return; }
-    L.small[2 * r] = (u32)s;
-    L.small[2 * r + 1] = (u32)e;
-  } else {
-    const u32 r = atomicAdd(&L.counts[1], 1u);
-    if (r >= L.cap_medium) { atomicOr(&L.counts[2], FIX_MEDIUM_FULL); return; }
-    L.medium[2 * r] = (u32)s;
-    L.medium[2 * r + 1] = (u32)e;
-  }
-}
-
-// Lists the runs of equal predicted position that start in this CTA's tile
-// and contain an inversion.
-// First set bit of the bitmap w in [lo, hi), or hi: a word at a time.
-__device__ __forceinline__ u32 first_bit_in(const u32* w, u32 lo, u32 hi) {
-  for (u32 q = lo; q < hi;) {
-    const u32 bits = w[q >> 5] >> (q & 31);
-    if (bits) {
-      const u32 r = q + __ffs(bits) - 1;
-      return r < hi ? r : hi;
-    }
-    q = (q | 31) + 1;
-  }
-  return hi;
-}
-
-__global__ void __launch_bounds__(kFindThreads) k_fix_find(u64* keys, u32* vals, const u32* spos, u64 n,
-                                                           FixLists L) {
-  __shared__ u64 sk[kFindTile + 1];
-  __shared__ u32 sp[kFindTile + 1];
-  __shared__ u32 sv[kFindTile + 1];
-  __shared__ u32 fb[kFindTile / 32 + 2], ib[kFindTile / 32 + 2];
-  __shared__ int s_open;
-  const u64 t0 = (u64)blockIdx.x * kFindTile;
-  const u64 t1 = min(n, t0 + kFindTile);
-  const u64 base = t0 ? t0 - 1 : 0;
-  const u32 len = (u32)(t1 - base);  // window: [base, t1)
-  for (u32 i = threadIdx.x; i < len; i += kFindThreads) {
-    sk[i] = keys[base + i];
-    sp[i] = spos[base + i];
-  }
-  if (threadIdx.x == 0) s_open = -1;
-  __syncthreads();
-  // bit i of fb: window position i starts a run; of ib: it is an inversion
-  const int lane = threadIdx.x & 31;
-  for (u32 w0 = (threadIdx.x >> 5) * 32; w0 < len; w0 += kFindThreads) {
-    const u32 i = w0 + lane;
-    bool f = false, v = false;
-    if (i < len) {
-      if (base + i == 0) f = true;
-      else if (i > 0) {
-        f = sp[i] != sp[i - 1];
-        v = !f && sk[i - 1] > sk[i];
-      }
-    }
-    const u32 bf = __ballot_sync(0xffffffffu, f), bi = __ballot_sync(0xffffffffu, v);
-    if (lane == 0) {
-      fb[w0 >> 5] = bf;
-      ib[w0 >> 5] = bi;
-    }
-  }
-  __syncthreads();
-  const u32 off = t0 ? 1u : 0u;
-  const u32 nwords = (len + 31) >> 5;
-  if (threadIdx.x == 0) {
-    // tile summary: last run start, and the first inversion of the run that
-    // was carried in from earlier tiles (positions before the first start)
-    u32 first = len, lastp = 0xffffffffu;
-    for (u32 w = 0; w < nwords; ++w) {
-      u32 b = fb[w];
-      if (w == 0 && off) b &= ~1u;
-      if (b) {
-        if (first == len) first = (w << 5) + __ffs(b) - 1;
-        lastp = (w << 5) + 31 - __clz(b);
-      }
-    }
-    const u32 cq = first_bit_in(ib, off, first);
-    const u32 cinv = cq < first ? cq : 0xffffffffu;
-    L.last_start[blockIdx.x] = lastp == 0xffffffffu ? lastp : (u32)(base + lastp);
-    L.carried_inv[blockIdx.x] = cinv == 0xffffffffu ? cinv : (u32)(base + cinv);
-  }
-  for (u32 i = off + threadIdx.x; i < len; i += kFindThreads) {
-    if (!((fb[i >> 5] >> (i & 31)) & 1u)) continue;
-    // next run start after i inside the window
-    u32 e = len;
-    u32 w = i >> 5;
-    u32 bits = fb[w] & ~((2u << (i & 31)) - 1u);
-    if ((i & 31) == 31) bits = 0;
-    while (true) {
-      if (bits) {
-        e = (w << 5) + __ffs(bits) - 1;
-        break;
-      }
-      if (++w >= nwords) break;
-      bits = fb[w];
-    }
-    if (e > len) e = len;
-    if (e == len && t1 < n) {  // continues past the tile: finished by warp 0
-      s_open = (int)i;
-      continue;
-    }
-    if (first_bit_in(ib, i + 1, e) >= e) continue;  // no inversion in the run
-    if (e - i > (u32)kFixSmall) {
-      fix_record(L, base + i, base + e);
-      continue;
-    }
-    // a short run inside the window: stable insertion sort here, then write back
-    for (u32 q = i; q < e; ++q) sv[q] = vals[base + q];
-    for (u32 q = i + 1; q < e; ++q) {
-      const u64 k = sk[q];
-      const u32 v = sv[q];
-      u32 r = q;
-      while (r > i && sk[r - 1] > k) {
-        sk[r] = sk[r - 1];
-        sv[r] = sv[r - 1];
-        --r;
-      }
-      sk[r] = k;
-      sv[r] = v;
-    }
-    for (u32 q = i; q < e; ++q) {
-      keys[base + q] = sk[q];
-      vals[base + q] = sv[q];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) L.scanned_to[blockIdx.x] = (u32)t1;
-  if (s_open < 0 || threadIdx.x >= 32) return;
-  // the last run of the tile continues past it: scan on, 32 keys at a time.
-  // A run whose keys are all equal so far holds no inversion; past
-  // kFixMaxRun such a run is left to k_fix_check.  A run with distinct keys
-  // is scanned to its end (at most kFixLongMax).
-  const u32 i = (u32)s_open;
-  const u32 p0 = sp[i];
-  const u64 k0 = sk[i];
-  bool inv = first_bit_in(ib, i + 1, len) < len, distinct = false;
-  for (u32 q = i + 1 + lane; q < len; q += 32) distinct |= sk[q] != k0;
-  distinct = __any_sync(0xffffffffu, distinct);
-  u64 prev_key = sk[len - 1];
-  u64 pos = t1;
-  u64 e = n;
-  bool ended = false;
-  constexpr int CH = 8;  // 32-key chunks loaded per round trip
-  bool done = false;
-  while (pos < n && !done) {
-    u64 kc[CH];
-    bool sc[CH];
 #pragma unroll
-    for (int c = 0; c < CH; ++c) {
-      const u64 q = pos + 32 * c + lane;
-      kc[c] = q < n ? keys[q] : 0;
-      sc[c] = q < n && spos[q] == p0;
-    }
-#pragma unroll
-    for (int c = 0; c < CH; ++c) {
-      if (done || pos >= n) break;
-      const u64 k = kc[c];
-      const u32 bs = __ballot_sync(0xffffffffu, sc[c]);
-      const u64 kp = __shfl_up_sync(0xffffffffu, k, 1);
-      const u64 km = lane == 0 ? prev_key : kp;
-      const u32 run_lanes = ~bs ? (u32)(__ffs(~bs) - 1) : 32u;
-      const bool mine = (u32)lane < run_lanes;
-      inv |= __ballot_sync(0xffffffffu, mine && km > k) != 0;
-      distinct |= __ballot_sync(0xffffffffu, mine && k != k0) != 0;
-      if (run_lanes < 32) {
-        e = pos + run_lanes;
-        ended = true;
-        done = true;
-        break;
-      }
-      prev_key = __shfl_sync(0xffffffffu, k, 31);
-      pos += 32;
-      const u64 scanned = pos - (base + i);
-      if ((!distinct && !inv && scanned > (u64)kFixMaxRun) || scanned > (u64)kFixLongMax) {
-        e = pos;
-        done = true;
-        break;
-      }
-    }
+  for (int o = 16; o; o >>= 1) {
+    const u64 a2 = __shfl_xor_sync(0xffffffffu, mn, o), b2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mn = a2 < mn ? a2 : mn;
+    mx = b2 > mx ? b2 : mx;
   }
-  if (pos >= n) ended = true;
   if (lane == 0) {
-    L.scanned_to[blockIdx.x] = (u32)(ended ? n : e);
-    if (inv) fix_record(L, base + i, ended ? e : (u64)n + kFixLongMax);  // unended + inversion: too long
+    red[warp] = mn;
+    red[warps + warp] = mx;
   }
+  __syncthreads();
+  mn = red[0];
+  mx = red[warps];
+  for (int w = 1; w < warps; ++w) {
+    mn = red[w] < mn ? red[w] : mn;
+    mx = red[warps + w] > mx ? red[warps + w] : mx;
+  }
+  __syncthreads();
 }
 
-// A run carried into a tile with an inversion the run's owner did not scan
-// (more than kFixMaxRun past the run start) means overflow.
-__global__ void k_fix_check(u64 tiles, FixLists L) {
-  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += (u64)gridDim.x * blockDim.x) {
-    const u32 inv = L.carried_inv[t];
-    if (inv == 0xffffffffu) continue;
-    u32 start = 0xffffffffu;
-    for (u64 k = 1; k <= t && k <= (u64)(kFixLongMax / kFindTile + 2); ++k) {
-      start = L.last_start[t - k];
-      if (start != 0xffffffffu) break;
-    }
-    // the owner of the run is the nearest earlier tile with a run start; it
-    // scanned the run up to scanned_to (its inversions there are handled)
-    u32 owner_scan = 0;
-    for (u64 k = 1; k <= t && k <= (u64)(kFixLongMax / kFindTile + 2); ++k)
-      if (L.last_start[t - k] != 0xffffffffu) {
-        owner_scan = L.scanned_to[t - k];
-        break;
-      }
-    if (start == 0xffffffffu || inv >= owner_scan) atomicOr(&L.counts[2], FIX_LONG_RUN);
-  }
-}
+constexpr size_t kBucketSmem = (size_t)kBucketCap * (8 + 4) + (size_t)2 * 8 * 256 * 4 + 256 * 4 + 32 * 4 + 16 * 8;
 
-// Sorts each short run by key with one warp (rank counting).
-__global__ void __launch_bounds__(256) k_fix_small(u64* keys, u32* vals, FixLists L) {
-  const u32 cnt = min(L.counts[0], L.cap_small);
-  const int lane = threadIdx.x & 31;
-  for (u64 r = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < cnt; r += ((u64)gridDim.x * blockDim.x) >> 5) {
-    const u32 s = L.small[2 * r], e = L.small[2 * r + 1];
-    const u32 m = e - s;
-    u64 k = 0;
-    u32 v = 0;
-    if ((u32)lane < m) {
-      k = keys[s + lane];
-      v = vals[s + lane];
-    }
-    u32 rank = 0;
-    for (u32 q = 0; q < m; ++q) {
-      const u64 kq = __shfl_sync(0xffffffffu, k, q);
-      rank += (kq < k) || (kq == k && q < (u32)lane);
-    }
-    __syncwarp();
-    if ((u32)lane < m) {
-      keys[s + rank] = k;
-      vals[s + rank] = v;
-    }
-  }
-}
-
-// Sorts each medium run with a block-wide stable LSD radix sort in shared
-// memory (8-bit digits of key - min over bit_length(max - min) bits).
-constexpr int kFixMedThreads = 256;
-__global__ void __launch_bounds__(kFixMedThreads) k_fix_medium(u64* keys, u32* vals, FixLists L) {
+// One bucket at a time per CTA: a stable LSD radix sort of key - min in
+// shared memory over bit_length(max - min) bits, 8 bits per pass.  Warp w
+// owns the bucket's rows [w * seg, (w + 1) * seg), seg = ceil(m / 8); item i
+// of lane l is row w * seg + 32 i + l, so (warp, item, lane) order is row
+// order and the warp ranking keeps equal digits in row order.
+__global__ void __launch_bounds__(kBucketThreads, 2) k_bucket_sort(BucketArgs a) {
+  constexpr int IPT = kBucketIPT, RADIX = 256, WARPS = kBucketThreads / 32;
   extern __shared__ __align__(16) unsigned char smem[];
-  u64* ka = (u64*)smem;                  // [kFixMaxRun]
-  u64* kb = ka + kFixMaxRun;             // [kFixMaxRun]
-  uint16_t* ia = (uint16_t*)(kb + kFixMaxRun);  // [kFixMaxRun] local indices
-  uint16_t* ib2 = ia + kFixMaxRun;
-  u32* sv = (u32*)(ib2 + kFixMaxRun);    // [kFixMaxRun] values
-  u32* wh = sv + kFixMaxRun;             // [8][256]
-  u32* tot = wh + 8 * 256;               // [256]
-  __shared__ u64 s_min, s_max;
-  __shared__ u32 scan_scratch[32];
+  u64* skeys = (u64*)smem;                       // [kBucketCap]
+  u32* sids = (u32*)(skeys + kBucketCap);        // [kBucketCap]
+  u32* whist = sids + kBucketCap;                // [WARPS][RADIX] counters
+  u32* wmask = whist + WARPS * RADIX;            // [WARPS][RADIX] peer masks
+  u32* sexcl = wmask + WARPS * RADIX;            // [RADIX]
+  u32* sscan = sexcl + RADIX;                    // [32]
+  u64* sred = (u64*)(sscan + 32);                // [16] per-warp min / max
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const u32 cnt = min(L.counts[1], L.cap_medium);
-  for (u32 r = blockIdx.x; r < cnt; r += gridDim.x) {
-    const u32 s = L.medium[2 * r], e = L.medium[2 * r + 1];
-    const u32 m = e - s;
-    if (tid == 0) {
-      s_min = ~0ull;
-      s_max = 0;
+  for (int i = tid; i < WARPS * RADIX; i += kBucketThreads) wmask[i] = 0u;
+  for (u32 b = blockIdx.x; b < a.nb; b += gridDim.x) {
+    const u32 s = a.starts[b], e = a.starts[b + 1], m = e - s;
+    if (m <= 1) continue;
+    if (m > kBucketCap) {  // listed for k_bucket_sort_large or the host
+      if (tid == 0) {
+        const u32 r = atomicAdd(&a.counts[0], 1u);
+        if (r < kBucketLargeMax) {
+          a.large[2 * r] = s;
+          a.large[2 * r + 1] = e;
+        }
+      }
+      continue;
+    }
+    const u32 seg = (m + WARPS - 1) / WARPS;
+    const u32 w0 = min(m, warp * seg), wn = min(seg, m - w0);  // this warp's rows [w0, w0 + wn)
+    u64 k[IPT];
+    u32 id[IPT];
+    u64 mn = ~0ull, mx = 0ull;
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 r = i * 32 + lane;
+      const bool in = r < wn;
+      k[i] = in ? a.keys[s + w0 + r] : 0ull;
+      id[i] = in ? a.ids[s + w0 + r] : 0u;
+      if (in) {
+        mn = k[i] < mn ? k[i] : mn;
+        mx = k[i] > mx ? k[i] : mx;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const u64 a2 = __shfl_xor_sync(0xffffffffu, mn, o), b2 = __shfl_xor_sync(0xffffffffu, mx, o);
+      mn = a2 < mn ? a2 : mn;
+      mx = b2 > mx ? b2 : mx;
+    }
+    if (lane == 0) {
+      sred[warp] = mn;
+      sred[WARPS + warp] = mx;
     }
     __syncthreads();
-    u64 lmin = ~0ull, lmax = 0;
-    for (u32 j = tid; j < m; j += kFixMedThreads) {
-      const u64 k = keys[s + j];
-      ka[j] = k;
-      ia[j] = (uint16_t)j;
-      sv[j] = vals[s + j];
-      lmin = k < lmin ? k : lmin;
-      lmax = k > lmax ? k : lmax;
+    mn = sred[0];
+    mx = sred[WARPS];
+#pragma unroll
+    for (int w = 1; w < WARPS; ++w) {
+      mn = sred[w] < mn ? sred[w] : mn;
+      mx = sred[WARPS + w] > mx ? sred[WARPS + w] : mx;
     }
-    atomicMin(&s_min, lmin);
-    atomicMax(&s_max, lmax);
-    __syncthreads();
-    const u64 mn = s_min;
-    const int bits = bit_length(s_max - mn);
-    const u32 seg = (m + 7) / 8;  // warp w sorts positions [w*seg, (w+1)*seg) in order
-    u64 *src = ka, *dst = kb;
-    uint16_t *isrc = ia, *idst = ib2;
+    const int bits = bit_length(mx - mn);
+    __syncthreads();  // sred is read by all before the next bucket writes it
+    if (bits == 0) continue;  // one key: the rows are in row order already
+    u32* wh = whist + warp * RADIX;
     for (int sh = 0; sh < bits; sh += 8) {
-      for (int i = tid; i < 8 * 256; i += kFixMedThreads) wh[i] = 0;
+      for (int i = lane; i < RADIX; i += 32) wh[i] = 0u;
+      __syncwarp();
+      u32 rd[IPT];
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) rd[i] = (u32)(i * 32 + lane) < wn ? (u32)((k[i] - mn) >> sh) & 255u : (u32)RADIX;
+      warp_rank_or<IPT, RADIX>(rd, wh, wmask + warp * RADIX, lane);
       __syncthreads();
-      const u32 w0 = warp * seg, w1 = min(m, w0 + seg);
-      for (u32 j = w0 + lane; j < w1; j += 32) atomicAdd(&wh[warp * 256 + (u32)(((src[j] - mn) >> sh) & 255u)], 1u);
-      __syncthreads();
-      for (int d = tid; d < 256; d += kFixMedThreads) {
+      // per digit: exclusive prefix over warps, then over digits
+      {
+        const int d = tid;  // RADIX == threads
         u32 run = 0;
-        for (int w = 0; w < 8; ++w) {
-          const u32 c = wh[w * 256 + d];
-          wh[w * 256 + d] = run;
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+          const u32 c = whist[w * RADIX + d];
+          whist[w * RADIX + d] = run;
           run += c;
         }
-        tot[d] = run;
+        sexcl[d] = run;
       }
       __syncthreads();
-      block_exclusive_scan<kFixMedThreads, 256>(tot, scan_scratch);
-      for (int d = tid; d < 256; d += kFixMedThreads)
-        for (int w = 0; w < 8; ++w) wh[w * 256 + d] += tot[d];
-      __syncthreads();
-      const u32 lt = lanemask_lt(), gt = lanemask_gt();
-      for (u32 j0 = w0; j0 < w1; j0 += 32) {
-        const u32 j = j0 + lane;
-        const bool in = j < w1;
-        const u32 d = in ? (u32)(((src[j] - mn) >> sh) & 255u) : 256u;
-        // lanes with the same digit: one ballot per digit bit (faster than
-        // match.any here); lanes past the segment end form their own group
-        u32 peers = __ballot_sync(0xffffffffu, in);
-        if (!in) peers = ~peers;
+      block_exclusive_scan<kBucketThreads, RADIX>(sexcl, sscan);
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const u32 bit = (d >> b) & 1u;
-          const u32 bb = __ballot_sync(0xffffffffu, bit);
-          peers &= bit ? bb : ~bb;
-        }
-        const u32 prior = in ? wh[warp * 256 + d] : 0u;
-        const u32 dst_i = prior + __popc(peers & lt);
-        __syncwarp();
-        if (in && !(peers & gt)) wh[warp * 256 + d] = prior + __popc(peers);
-        __syncwarp();
-        if (in) {
-          dst[dst_i] = src[j];
-          idst[dst_i] = isrc[j];
+      for (int i = 0; i < IPT; ++i) {
+        if (rd[i] != kNoRank) {
+          const u32 d = rd[i] >> 16;
+          const u32 slot = sexcl[d] + wh[d] + (rd[i] & 0xffffu);
+          skeys[slot] = k[i];
+          sids[slot] = id[i];
         }
       }
       __syncthreads();
-      u64* t = src;
-      src = dst;
-      dst = t;
-      uint16_t* ti = isrc;
-      isrc = idst;
-      idst = ti;
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        const u32 r = i * 32 + lane;
+        if (r < wn) {
+          k[i] = skeys[w0 + r];
+          id[i] = sids[w0 + r];
+        }
+      }
+      __syncthreads();  // skeys / whist are rewritten by the next pass
     }
-    for (u32 j = tid; j < m; j += kFixMedThreads) {
-      keys[s + j] = src[j];
-      vals[s + j] = sv[isrc[j]];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 r = i * 32 + lane;
+      if (r < wn) {
+        a.keys[s + w0 + r] = k[i];
+        a.ids[s + w0 + r] = id[i];
+      }
     }
-    __syncthreads();
   }
 }
 
-// Sorts each long run (kFixMaxRun < length <= kFixLongMax) with one CTA: a
-// stable LSD radix sort of 8-bit digits of key - min, ping-ponging between
-// the run's place in the output and the same positions of a scratch array.
-__global__ void __launch_bounds__(kFixMedThreads) k_fix_long(u64* keys, u32* vals, u64* tkeys, u32* tvals,
-                                                             FixLists L) {
-  __shared__ u32 hist[256];
-  __shared__ u32 wh[8][256];
-  __shared__ u64 s_min, s_max;
-  __shared__ u32 scan_scratch[32];
+struct LargeArgs {
+  u64* keys;           // in/out (the bucket's rows)
+  u32* ids;
+  u64* tkeys;          // scratch, same positions
+  u32* tids;
+  const u32* large;    // [count][2] (start, end)
+  const u32* counts;   // [0] listed buckets (at most kBucketLargeMax are in the list)
+};
+
+// Listed large buckets of at most kLargeCtaMax rows, one CTA each: min and
+// max of the bucket's keys, then a stable LSD radix sort of key - min, 8 bits
+// per pass, through the scratch arrays (a bucket of one key is left as is).
+// Per pass a counting read gives each digit's first position; then chunks of
+// kBucketCap rows in row order are ranked as in k_bucket_sort (warp w owns
+// rows [512 w, 512 w + 512) of the chunk) and written to the digit's next
+// positions, so equal digits keep row order across chunks.
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(LargeArgs a) {
+  constexpr int IPT = kBucketIPT, RADIX = 256, WARPS = kBucketThreads / 32, SEG = 32 * IPT;
+  __shared__ u32 whist[WARPS * RADIX];
+  __shared__ u32 wmask[WARPS * RADIX];
+  __shared__ u32 sbase[RADIX], stot[RADIX], sscan[32];
+  __shared__ u64 sred[2 * WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const u32 cnt = min(L.counts[3], L.cap_long);
-  for (u32 r = blockIdx.x; r < cnt; r += gridDim.x) {
-    const u32 s = L.lng[2 * r], e = L.lng[2 * r + 1];
-    if (tid == 0) {
-      s_min = ~0ull;
-      s_max = 0;
-    }
-    __syncthreads();
-    u64 lmin = ~0ull, lmax = 0;
-    for (u32 j = s + tid; j < e; j += kFixMedThreads) {
-      const u64 k = keys[j];
-      lmin = k < lmin ? k : lmin;
-      lmax = k > lmax ? k : lmax;
-    }
-    atomicMin(&s_min, lmin);
-    atomicMax(&s_max, lmax);
-    __syncthreads();
-    const u64 mn = s_min;
-    const int bits = bit_length(s_max - mn);
-    u64 *ks = keys, *kd = tkeys;
-    u32 *vs = vals, *vd = tvals;
+  for (int i = tid; i < WARPS * RADIX; i += kBucketThreads) wmask[i] = 0u;
+  const u32 count = min(a.counts[0], kBucketLargeMax);
+  for (u32 r = blockIdx.x; r < count; r += gridDim.x) {
+    const u32 s = a.large[2 * r], e = a.large[2 * r + 1];
+    if (e - s > kLargeCtaMax) continue;  // the host sorts it
+    u64 mn, mx;
+    block_minmax(a.keys, s, e, sred, mn, mx);
+    const int bits = bit_length(mx - mn);  // 0: one key, the rows are in row order already
+    u64* ks = a.keys;
+    u32* is = a.ids;
+    u64* kd = a.tkeys;
+    u32* id = a.tids;
     for (int sh = 0; sh < bits; sh += 8) {
-      for (int i = tid; i < 256; i += kFixMedThreads) hist[i] = 0;
+      sbase[tid] = 0u;
       __syncthreads();
-      for (u32 j = s + tid; j < e; j += kFixMedThreads) atomicAdd(&hist[(u32)(((ks[j] - mn) >> sh) & 255u)], 1u);
+      for (u32 j = s + tid; j < e; j += kBucketThreads) atomicAdd(&sbase[(u32)((ks[j] - mn) >> sh) & 255u], 1u);
       __syncthreads();
-      block_exclusive_scan<kFixMedThreads, 256>(hist, scan_scratch);  // hist: running base per digit
-      // chunks of 256 rows in order; inside a chunk, warp w takes rows
-      // [w*32, w*32+32) so warps are in row order too
-      const u32 lt = lanemask_lt();
-      for (u32 c0 = s; c0 < e; c0 += kFixMedThreads) {
-        for (int i = tid; i < 8 * 256; i += kFixMedThreads) (&wh[0][0])[i] = 0;
-        __syncthreads();
-        const u32 j = c0 + tid;
-        const bool in = j < e;
-        const u64 k = in ? ks[j] : 0;
-        const u32 v = in ? vs[j] : 0;
-        const u32 d = in ? (u32)(((k - mn) >> sh) & 255u) : 256u;
-        u32 peers = __ballot_sync(0xffffffffu, in);
-        if (!in) peers = ~peers;
+      block_exclusive_scan<kBucketThreads, RADIX>(sbase, sscan);
+      u32* wh = whist + warp * RADIX;
+      for (u32 c0 = s; c0 < e; c0 += kBucketCap) {
+        for (int i = lane; i < RADIX; i += 32) wh[i] = 0u;
+        __syncwarp();
+        const u32 w0 = c0 + warp * SEG;
+        u64 k[IPT];
+        u32 v[IPT], rd[IPT];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const u32 bit = (d >> b) & 1u;
-          const u32 bb = __ballot_sync(0xffffffffu, bit);
-          peers &= bit ? bb : ~bb;
+        for (int i = 0; i < IPT; ++i) {
+          const u32 j = w0 + i * 32 + lane;
+          const bool in = j < e && j >= w0;  // j >= w0 guards the 32-bit wrap
+          k[i] = in ? ks[j] : 0ull;
+          v[i] = in ? is[j] : 0u;
+          rd[i] = in ? (u32)((k[i] - mn) >> sh) & 255u : (u32)RADIX;
         }
-        const u32 rank = __popc(peers & lt);
-        if (in && !(peers & lanemask_gt())) wh[warp][d] = __popc(peers);
+        warp_rank_or<IPT, RADIX>(rd, wh, wmask + warp * RADIX, lane);
         __syncthreads();
-        // offset of this warp's first row of digit d: earlier warps of the chunk
-        u32 before = 0;
-        if (in)
-          for (int w = 0; w < warp; ++w) before += wh[w][d];
-        if (in) {
-          const u32 dst = s + hist[d] + before + rank;
-          kd[dst] = k;
-          vd[dst] = v;
+        {
+          u32 run = 0;
+#pragma unroll
+          for (int w = 0; w < WARPS; ++w) {
+            const u32 c = whist[w * RADIX + tid];
+            whist[w * RADIX + tid] = run;
+            run += c;
+          }
+          stot[tid] = run;
         }
         __syncthreads();
-        if (tid < 256) {
-          u32 tot = 0;
-          for (int w = 0; w < 8; ++w) tot += wh[w][tid];
-          hist[tid] += tot;
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+          if (rd[i] != kNoRank) {
+            const u32 d = rd[i] >> 16;
+            const u32 dst = s + sbase[d] + wh[d] + (rd[i] & 0xffffu);
+            kd[dst] = k[i];
+            id[dst] = v[i];
+          }
         }
+        __syncthreads();
+        sbase[tid] += stot[tid];
         __syncthreads();
       }
       u64* tk = ks;
       ks = kd;
       kd = tk;
-      u32* tv = vs;
-      vs = vd;
-      vd = tv;
+      u32* tv = is;
+      is = id;
+      id = tv;
     }
-    if (ks != keys) {  // odd number of passes: the run ended up in the scratch
-      for (u32 j = s + tid; j < e; j += kFixMedThreads) {
-        keys[j] = ks[j];
-        vals[j] = vs[j];
+    if (ks != a.keys) {  // an odd number of passes left the rows in the scratch
+      for (u32 j = s + tid; j < e; j += kBucketThreads) {
+        a.keys[j] = ks[j];
+        a.ids[j] = is[j];
       }
     }
     __syncthreads();
   }
 }
-
-constexpr size_t kFixMediumSmem = (size_t)kFixMaxRun * (8 + 8 + 2 + 2 + 4) + (8 * 256 + 256) * 4;
 
 }  // namespace jfx

@@ -23,6 +23,9 @@
 
 namespace jfx {
 
+// No tile (tile ids stay below 2^30).
+constexpr u32 kNoTile = 0xffffffffu;
+
 // look-back status word: [31:30] flag, [29:0] count
 constexpr u32 ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_ERR = 3u << 30, ST_CNT = (1u << 30) - 1;
 
@@ -48,8 +51,60 @@ struct PassLayout {
   static constexpr size_t PAY_BYTES = (size_t)NW * TILE * 4;  // payload staged in row order
   static constexpr size_t IDX_BYTES = (size_t)TILE * 2;       // sorted slot -> staging slot
   static constexpr size_t DIG_BYTES = (size_t)TILE * 2;
-  static constexpr size_t SMEM = A_BYTES + PAY_BYTES + IDX_BYTES + DIG_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
+  // Ranking by per-warp peer masks in shared memory (OR_RANK, digits of up to
+  // 9 bits) or by one ballot per digit bit (wider digits, whose mask rows
+  // would not fit).  The mask rows live only during the ranking and share
+  // their bytes with the slot and digit arrays written after it.
+  static constexpr bool OR_RANK = RB <= 9;
+  static constexpr size_t MASK_BYTES = OR_RANK ? (size_t)WARPS * RADIX * 4 : 0;
+  static constexpr size_t R_BYTES =
+      MASK_BYTES > IDX_BYTES + DIG_BYTES ? MASK_BYTES : IDX_BYTES + DIG_BYTES;
+  static constexpr size_t SMEM = A_BYTES + PAY_BYTES + R_BYTES + 2 * (size_t)RADIX * 4 + 64 * 4;
 };
+
+// Stable rank of each item among the warp's items of the same digit.  Item i
+// of lane l is row 32 i + l of the warp's rows, so (item, lane) order is row
+// order.  wh: this warp's counter row (wh[d] = the digit's items already
+// counted; advanced here); wm: this warp's mask row, zero on entry and left
+// zero.  Lanes of one digit set their bits in wm[d] with a shared-memory OR,
+// read the peer mask back, and the highest peer advances wh[d] for the group
+// and clears wm[d].  A warp whose valid items share one digit (sorted or
+// constant keys, where the ORs would all hit one word) takes a shortcut.
+// In place: rd[i] is the item's digit on entry (RADIX: no item) and on exit
+// (digit << 16) | (counter value before the item + its rank among its
+// peers), or kNoRank for no item.
+constexpr u32 kNoRank = 0xffffffffu;
+template <int IPT, int RADIX>
+__device__ __forceinline__ void warp_rank_or(u32 (&rd)[IPT], u32* wh, u32* wm, int lane) {
+  const u32 lt = lanemask_lt(), bit = 1u << lane;
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 d = rd[i];
+    const bool valid = d < (u32)RADIX;
+    const u32 d0 = __shfl_sync(0xffffffffu, d, 0);
+    u32 rank;
+    if (__all_sync(0xffffffffu, d == d0)) {
+      // one digit for the whole warp (or no valid item at all)
+      const u32 before = valid ? wh[d] : 0u;
+      __syncwarp();
+      if (valid && lane == 31) wh[d] = before + 32u;
+      rank = before + (u32)lane;
+    } else {
+      if (valid) atomicOr(&wm[d], bit);
+      __syncwarp();
+      const u32 peers = valid ? wm[d] : 0u;
+      const u32 before = valid ? wh[d] : 0u;
+      __syncwarp();
+      if (valid && (peers >> lane) == 1u) {
+        wm[d] = 0u;
+        wh[d] = before + (u32)__popc(peers);
+      }
+      rank = before + (u32)__popc(peers & lt);
+    }
+    __syncwarp();
+    rd[i] = valid ? (d << 16) | rank : kNoRank;
+  }
+}
 
 // Where the first pass reads payload word w of row r: *(u32*)(ptr + r*stride + off);
 // a null ptr means the row id itself.
@@ -165,7 +220,7 @@ struct PassArgs {
   // prefix over earlier tiles only)
   const u32* digit_starts;
   u64 spin_ns;        // bound of each look-back wait
-  u32 withhold_tile;  // failure injection: this look-back ticket publishes nothing (0: none)
+  u32 withhold_tile;  // failure injection: this look-back ticket publishes nothing (kNoTile: none)
 };
 
 __device__ __forceinline__ u32 fmix32(u32 h) {
@@ -367,7 +422,8 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   u32* spay = (u32*)(smem + L::A_BYTES);                 // [NW][TILE] payload, row order
   uint16_t* sidx = (uint16_t*)(smem + L::A_BYTES + L::PAY_BYTES);  // sorted slot -> row slot
   uint16_t* sdig = sidx + TILE;      // digit of each sorted slot
-  u32* sexcl = (u32*)(sdig + TILE);  // tile digit counts, then the tile's exclusive prefix
+  u32* wmask = (u32*)sidx;           // [WARPS][RADIX] peer masks during the ranking (OR_RANK)
+  u32* sexcl = (u32*)(smem + L::A_BYTES + L::PAY_BYTES + L::R_BYTES);  // tile digit counts, then the tile's exclusive prefix
   u32* sbase = sexcl + RADIX;        // global position of the tile's first key of each digit
   u32* sscan = sbase + RADIX;        // 32 words of block-scan scratch
   u32* sflag = sscan + 32;           // [0] tile id, [1] abort
@@ -378,6 +434,19 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     sflag[1] = 0;
   }
   for (int i = tid; i < WARPS * RADIX; i += THREADS) whist[i] = 0u;
+  if constexpr (L::OR_RANK)
+    for (int i = tid; i < WARPS * RADIX; i += THREADS) wmask[i] = 0u;
+  // two-phase pass: this tile's global digit bases do not depend on the
+  // tile's keys; their loads go out now, ahead of the key loads' use
+  constexpr int DPT = RADIX >= THREADS ? RADIX / THREADS : 1;  // digits per thread
+  u32 tb_pre[DPT];
+  if constexpr (TP) {
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) {
+      const int d = tid + k * THREADS;
+      tb_pre[k] = d < RADIX ? __ldg(a.digit_starts + d) + __ldg(a.tile_base + (u64)d * a.ntiles + blockIdx.x) : 0u;
+    }
+  }
   __syncthreads();
   const u32 tile = sflag[0];
   // segment of the tile: rows [seg_row0, seg_row1), tiles from seg_tile0
@@ -577,25 +646,32 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     // reads the payload already moved to sorted order: no per-row count
     // atomics, digit or row-slot arrays in shared memory.
     u32* wh = whist + warp * RADIX;
-    const u32 lt = lanemask_lt();
+    if constexpr (L::OR_RANK) {
+      warp_rank_or<IPT, RADIX>(rd, wh, wmask + warp * RADIX, lane);
 #pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-      const u32 d = rd[i];
-      const bool valid = d < (u32)RADIX;
-      u32 peers = __ballot_sync(0xffffffffu, valid);
-      if (!valid) peers = ~peers;
+      for (int i = 0; i < IPT; ++i)
+        rd[i] = rd[i] != kNoRank ? 0x80000000u | ((rd[i] >> 16) << 13) | (rd[i] & 0xffffu) : 0u;
+    } else {
+      const u32 lt = lanemask_lt();
 #pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        const u32 bit = (d >> b) & 1u;
-        const u32 bb = __ballot_sync(0xffffffffu, bit);
-        peers &= bit ? bb : ~bb;
+      for (int i = 0; i < IPT; ++i) {
+        const u32 d = rd[i];
+        const bool valid = d < (u32)RADIX;
+        u32 peers = __ballot_sync(0xffffffffu, valid);
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < RB; ++b) {
+          const u32 bit = (d >> b) & 1u;
+          const u32 bb = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? bb : ~bb;
+        }
+        const int leader = 31 - __clz(peers);
+        u32 prior = 0;
+        if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
+        prior = __shfl_sync(0xffffffffu, prior, leader);
+        // bit 31 item present, bits [13, 24) digit, [0, 13) rank in the warp
+        rd[i] = valid ? 0x80000000u | (d << 13) | (prior + __popc(peers & lt)) : 0u;
       }
-      const int leader = 31 - __clz(peers);
-      u32 prior = 0;
-      if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
-      prior = __shfl_sync(0xffffffffu, prior, leader);
-      // bit 31 item present, bits [13, 24) digit, [0, 13) rank in the warp
-      rd[i] = valid ? 0x80000000u | (d << 13) | (prior + __popc(peers & lt)) : 0u;
     }
     __syncthreads();
     for (int d = tid; d < RADIX; d += THREADS) {
@@ -610,8 +686,11 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     }
     __syncthreads();
     block_exclusive_scan<THREADS, RADIX>(sexcl, sscan);  // tile-local start of each digit
-    for (int d = tid; d < RADIX; d += THREADS)
-      sbase[d] = (u32)seg_row0 + a.digit_starts[d] + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) {
+      const int d = tid + k * THREADS;
+      if (d < RADIX) sbase[d] = (u32)seg_row0 + tb_pre[k] - sexcl[d];
+    }
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
       if (rd[i] & 0x80000000u) {
@@ -762,25 +841,35 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   // keep row order.  Peers are found with one ballot per digit bit; the
   // lowest peer advances the warp's counter for the whole group.
   static_assert(TILE <= 8192 && RADIX <= 2048, "position/digit packing");
-  const u32 lt = lanemask_lt();
+  if constexpr (L::OR_RANK) {
+    warp_rank_or<IPT, RADIX>(rd, wh, wmask + warp * RADIX, lane);
 #pragma unroll
-  for (int i = 0; i < IPT; ++i) {
-    const u32 d = rd[i];
-    const bool valid = d < (u32)RADIX;
-    u32 peers = __ballot_sync(0xffffffffu, valid);
-    if (!valid) peers = ~peers;
-#pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const u32 bit = (d >> b) & 1u;
-      const u32 bb = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? bb : ~bb;
+    for (int i = 0; i < IPT; ++i) {
+      const u32 d = rd[i] >> 16;
+      // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
+      rd[i] = rd[i] != kNoRank ? 0x80000000u | (d << 13) | (sexcl[d] + (rd[i] & 0xffffu)) : 0u;
     }
-    const int leader = 31 - __clz(peers);
-    u32 prior = 0;
-    if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
-    prior = __shfl_sync(0xffffffffu, prior, leader);
-    // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
-    rd[i] = valid ? 0x80000000u | (d << 13) | (sexcl[d] + prior + __popc(peers & lt)) : 0u;
+  } else {
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      const u32 d = rd[i];
+      const bool valid = d < (u32)RADIX;
+      u32 peers = __ballot_sync(0xffffffffu, valid);
+      if (!valid) peers = ~peers;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) {
+        const u32 bit = (d >> b) & 1u;
+        const u32 bb = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bb : ~bb;
+      }
+      const int leader = 31 - __clz(peers);
+      u32 prior = 0;
+      if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
+      prior = __shfl_sync(0xffffffffu, prior, leader);
+      // rd becomes: bit 31 item present, bits [13, 25) digit, [0, 13) tile-local position
+      rd[i] = valid ? 0x80000000u | (d << 13) | (sexcl[d] + prior + __popc(peers & lt)) : 0u;
+    }
   }
   __syncthreads();  // whist reads above are done before skeys (aliased) is written
 #pragma unroll
@@ -1719,7 +1808,7 @@ inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles 
   int tiles = grid_tiles ? (int)grid_tiles : ceil_div(n, L::TILE);
   PassArgs pa = a;
   pa.spin_ns = (u64)g_tuning.spin_limit_us * 1000ull;
-  pa.withhold_tile = g_fault.withhold_tile > 0 ? (u32)g_fault.withhold_tile : 0u;
+  pa.withhold_tile = g_fault.withhold_tile > 0 ? (u32)g_fault.withhold_tile : kNoTile;
   const long t = timing_begin(s);
   k_onesweep<K, RB, FM, NW, TP><<<tiles, L::THREADS, L::SMEM, s>>>(pa), note_launch();
   if (t >= 0) {

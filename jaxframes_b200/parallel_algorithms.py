@@ -274,7 +274,10 @@ def _value_dtype_rules(v: torch.Tensor, agg: str, multi: bool):
     raise ValueError(f"Unsupported aggregation function: {agg}")
 
 
-def _run_groupby(keys, values: dict, agg_funcs: dict, multi: bool):
+def _run_groupby(keys, values: dict, agg_funcs: dict, multi: bool, rules=None):
+    """One jfx_groupby call.  ``rules(value, agg, multi)`` gives each output's
+    dtype (default: the reference module's rules)."""
+    rules = rules or _value_dtype_rules
     cols = [as_device(k) for k in keys]
     n = cols[0].numel()
     for c in cols:
@@ -294,7 +297,7 @@ def _run_groupby(keys, values: dict, agg_funcs: dict, multi: bool):
     agg_cols = []
     for col, agg in agg_funcs.items():
         v = vals[col]
-        odt = _value_dtype_rules(v, agg, multi)
+        odt = rules(v, agg, multi)
         out = _empty(n, odt, v)
         outputs[col] = out
         key = v.data_ptr()
@@ -592,7 +595,7 @@ def learned_sort(keys, mode: str = "auto"):
     ``(sorted_keys, perm int32, learned_used)``, identical to the plain radix
     sort.  ``mode``: "auto" (learned with plain fallback) or "plain".
     ``learned_used`` is 1 for the learned path, 0 for plain, negative for a
-    fallback (-1 model check, -2 run too long, -3 run list full)."""
+    fallback (-1 model check failed, -3 large-bucket list full)."""
     k = as_device(keys)
     if k.dtype != torch.uint64:
         raise TypeError(f"learned_sort takes uint64 keys, got {k.dtype}")

@@ -39,6 +39,9 @@ __all__ = [
     "hash_partition",
     "compact_repartitioned_rows",
     "default_float",
+    "groupby_encoded_strings",
+    "join_encoded_strings",
+    "sortable_string_codes",
 ]
 
 _FLOATS = (np.float32, np.float64)
@@ -439,3 +442,145 @@ def compact_repartitioned_rows(keys, values, valid_mask):
         return keys, values
     pos = np.flatnonzero(valid_mask)
     return [np.asarray(k)[pos] for k in keys], {n: np.asarray(a)[pos] for n, a in values.items()}
+
+
+# ------------------------------------------------ dictionary-encoded strings ---
+# core/string_fastpaths.py: string columns are int32 dictionary codes into a
+# lexicographically sorted vocabulary, null = -1 (core/string_encoding.py:37-51).
+
+def string_agg_dtype(vals: np.ndarray, agg: str):
+    """``_aggregation_output_dtype`` (string_fastpaths.py:151-157): mean is
+    ``result_type(dtype, float32)``, count int32, the rest the value dtype."""
+    if agg == "mean":
+        return np.float64 if vals.dtype == np.float64 else np.float32
+    if agg == "count":
+        return np.int32
+    return vals.dtype.type
+
+
+def groupby_encoded_strings(keys, values: dict, agg_funcs: dict, vocab_size: int):
+    """``groupby_encoded_strings`` (string_fastpaths.py:41-74) with
+    ``_aggregate_by_code`` (:160-184).  Null codes (< 0) are dropped; codes of
+    ``vocab_size`` or more are dropped too (``bincount(length=vocab_size)`` and
+    the scatters drop out-of-range indices).  Groups are the observed codes in
+    ascending order.  Sums accumulate in the value dtype (float sums here in
+    float64, rounded once; the reference's scatter-add order is unpinned);
+    mean = sum / count in the sum's dtype (integers: true division in the
+    default float); min/max propagate NaN."""
+    keys = np.asarray(keys)
+    valid = (keys >= 0) & (keys < vocab_size)
+    if not valid.any():
+        return (keys[:0].copy(),
+                {c: np.zeros(0, string_agg_dtype(np.asarray(values[c]), a)) for c, a in agg_funcs.items()})
+    vk = keys[valid].astype(np.int64)
+    counts = np.bincount(vk, minlength=vocab_size)[:vocab_size]
+    observed = counts > 0
+    codes = np.arange(vocab_size, dtype=keys.dtype)[observed]
+    seg_of_code = np.cumsum(observed) - 1
+    seg = seg_of_code[vk]
+    g = int(observed.sum())
+    cnt = counts[observed]
+    out = {}
+    for col, agg in agg_funcs.items():
+        v = np.asarray(values[col])[valid]
+        if agg == "count":
+            out[col] = cnt.astype(np.int32)
+        elif agg == "sum":
+            out[col] = _segment_sum(v, seg, g, v.dtype.type)
+        elif agg == "mean":
+            s = _segment_sum(v, seg, g, v.dtype.type)
+            od = string_agg_dtype(v, "mean")
+            out[col] = (s.astype(od) / cnt.astype(od)).astype(od)
+        elif agg in ("min", "max"):
+            out[col] = _segment_max(v, seg, g, agg == "min")
+        else:
+            raise ValueError(f"Unsupported aggregation function: {agg}")
+    return codes, out
+
+
+def _string_domain(codes, null_code):
+    c = np.asarray(codes)
+    return np.where(c < 0, null_code, c).astype(np.int32)
+
+
+def _restore_nulls(codes, null_code):
+    return np.where(codes == null_code, -1, codes).astype(np.int32)
+
+
+def join_encoded_strings(left_keys, right_keys, num_codes: int, how: str):
+    """``join_encoded_strings`` (string_fastpaths.py:95-119): null codes become
+    the extra code ``num_codes``, so nulls match nulls.  Returns
+    ``(joined_codes, left_indices, right_indices)`` (-1: no row).
+
+    Right side unique (every code at most once, :217-262): inner = matched left
+    rows in left row order; left = every left row in order; right = matched
+    left rows in order, then unmatched right rows ascending; outer = every left
+    row in order, then unmatched right rows ascending.
+
+    Otherwise (:265-309) codes ascending; per code the left-major cartesian
+    product of its left rows and right rows (each in row order), or for left /
+    right / outer joins the code's unmatched rows of one side."""
+    if how not in ("inner", "left", "right", "outer"):
+        raise ValueError(f"Unsupported join type: {how}")
+    null = int(num_codes)
+    ld = _string_domain(left_keys, null)
+    rd = _string_domain(right_keys, null)
+    size = null + 1
+    rc = np.bincount(rd, minlength=size)
+    nl, nr = len(ld), len(rd)
+    if (rc <= 1).all():
+        lookup = np.full(size, -1, dtype=np.int32)
+        lookup[rd] = np.arange(nr, dtype=np.int32)
+        lpos = np.arange(nl, dtype=np.int32)
+        mr = lookup[ld] if nl else np.zeros(0, np.int32)
+        ok = mr >= 0
+        if how == "inner":
+            return _restore_nulls(ld[ok], null), lpos[ok], mr[ok]
+        if how == "left":
+            return _restore_nulls(ld, null), lpos, mr
+        hit = np.zeros(nr, dtype=bool)
+        hit[mr[ok]] = True
+        un = np.flatnonzero(~hit).astype(np.int32)
+        neg = np.full(len(un), -1, dtype=np.int32)
+        if how == "right":
+            return (_restore_nulls(np.concatenate([ld[ok], rd[un]]), null), np.concatenate([lpos[ok], neg]),
+                    np.concatenate([mr[ok], un]))
+        return (_restore_nulls(np.concatenate([ld, rd[un]]), null), np.concatenate([lpos, neg]),
+                np.concatenate([mr, un]))
+    # several rows per code on the right: per code, in code order
+    lo = np.argsort(ld, kind="stable").astype(np.int32)
+    ro = np.argsort(rd, kind="stable").astype(np.int32)
+    lcnt = np.bincount(ld, minlength=size)
+    rcnt = np.bincount(rd, minlength=size)
+    lst = np.concatenate([[0], np.cumsum(lcnt)])
+    rst = np.concatenate([[0], np.cumsum(rcnt)])
+    codes, li, ri = [], [], []
+    for code in np.flatnonzero((lcnt > 0) | (rcnt > 0)):
+        L = lo[lst[code]:lst[code + 1]]
+        R = ro[rst[code]:rst[code + 1]]
+        if len(L) and len(R):
+            codes.append(np.full(len(L) * len(R), code, np.int32))
+            li.append(np.repeat(L, len(R)))
+            ri.append(np.tile(R, len(L)))
+        elif len(L) and how in ("left", "outer"):
+            codes.append(np.full(len(L), code, np.int32))
+            li.append(L)
+            ri.append(np.full(len(L), -1, np.int32))
+        elif len(R) and how in ("right", "outer"):
+            codes.append(np.full(len(R), code, np.int32))
+            li.append(np.full(len(R), -1, np.int32))
+            ri.append(R)
+    if not codes:
+        e = np.zeros(0, np.int32)
+        return e, e.copy(), e.copy()
+    return (_restore_nulls(np.concatenate(codes), null), np.concatenate(li).astype(np.int32),
+            np.concatenate(ri).astype(np.int32))
+
+
+def sortable_string_codes(codes, vocab_size: int, descending: bool = False):
+    """``sortable_string_codes`` (string_encoding.py:115-124): lexical order,
+    nulls last either way."""
+    c = np.asarray(codes)
+    if not descending:
+        return np.where(c < 0, vocab_size, c)
+    return np.where(c < 0, vocab_size, (vocab_size - 1) - c)
