@@ -96,25 +96,39 @@ struct GroupBuffers {
   u32* warp_base;
   u32* partial;
   u32* total;
-  u32* slot_gid;
-  u32* slot_started;
-  u64* slot_state;
+  u32* starts;  // [groups + 1] first row of each group
   u64 nwarps;
 };
+static void take_group_buffers(Arena& ar, u64 n, GroupBuffers& g) {
+  g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
+  g.warp_count = ar.take<u32>(g.nwarps + 1);
+  g.warp_base = ar.take<u32>(g.nwarps + 1);
+  g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
+  g.total = ar.take<u32>(4);
+  g.starts = ar.take<u32>(n + 1);
+}
 static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b, GroupBuffers& g) {
   take_common(ar, c);
   take_sort_buffers(ar, n, b, kMaxWords);
   g.sk = ar.take<u64>(n ? n : 1);
   g.perm = ar.take<u32>(n ? n : 1);
   for (int w = 0; w < kMaxWords; ++w) g.words[w] = ar.take<u32>(n ? n : 1);
-  g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
-  g.warp_count = ar.take<u32>(g.nwarps + 1);
-  g.warp_base = ar.take<u32>(g.nwarps + 1);
-  g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
-  g.total = ar.take<u32>(4);
-  g.slot_gid = ar.take<u32>(2 * g.nwarps + 1);
-  g.slot_started = ar.take<u32>(2 * g.nwarps + 1);
-  g.slot_state = ar.take<u64>((u64)std::max(nvals, 1) * 4 * (2 * g.nwarps + 1));
+  take_group_buffers(ar, n, g);
+}
+
+// Group boundaries, counts, first rows and key columns, then the
+// group-parallel reduction of every value column (groupby.cuh).  n >= 1.
+template <typename K>
+static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((g.nwarps * 32 + 255) / 256);
+  k_group_count<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
+  k_group_starts<K><<<blocks, 256, 0, s>>>(ga, g.nwarps, g.starts), note_launch();
+  k_group_end<<<1, 1, 0, s>>>(g.starts, g.total, n), note_launch();
+  k_group_agg<<<grid_for(n, 256), 256, 0, s>>>(ga, g.starts, g.total), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  return JFX_OK;
 }
 
 // ------------------------------------------------------------------- join ---
@@ -345,15 +359,7 @@ static void carve_batch(Arena& ar, u64 n, u64 nq, Common& c, BatchBuffers& b) {
   b.sk = ar.take<u32>(nn);
   b.sv = ar.take<u32>(nn);
   b.group_q = ar.take<u32>(nn);
-  GroupBuffers& g = b.g;
-  g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
-  g.warp_count = ar.take<u32>(g.nwarps + 1);
-  g.warp_base = ar.take<u32>(g.nwarps + 1);
-  g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
-  g.total = ar.take<u32>(4);
-  g.slot_gid = ar.take<u32>(2 * g.nwarps + 1);
-  g.slot_started = ar.take<u32>(2 * g.nwarps + 1);
-  g.slot_state = ar.take<u64>(4 * (2 * g.nwarps + 1));
+  take_group_buffers(ar, n, b.g);
 }
 
 // -------------------------------------------------------------- partition ---
@@ -844,21 +850,8 @@ int jfx_groupby(const jfx_column* keys, int ncols, int64_t n, int multi_key, con
   ga.warp_base = g.warp_base;
   ga.pack = kp.pack;
   for (int j = 0; j < ncols; ++j) ga.uniq_out[j] = unique_out ? unique_out[j] : nullptr;
-  ga.slot_gid = g.slot_gid;
-  ga.slot_started = g.slot_started;
-  ga.slot_state = g.slot_state;
-  ga.nslots = 2 * g.nwarps;
-  const unsigned blocks = (unsigned)((g.nwarps * 32 + 255) / 256);
-  if (rq.key64) k_group_count<u64><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
-  else k_group_count<u32><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
-  JFX_CUDA(cudaGetLastError());
-  JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
-  JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
-  if (rq.key64) k_group_reduce<u64><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
-  else k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
-  JFX_CUDA(cudaGetLastError());
-  k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
-  JFX_CUDA(cudaGetLastError());
+  if (rq.key64) JFX_TRY(launch_group_reduce<u64>(ga, g, (u64)n, s));
+  else JFX_TRY(launch_group_reduce<u32>(ga, g, (u64)n, s));
   u64* host = g_host.get();
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host + 1, g.total, sizeof(u32), cudaMemcpyDeviceToHost, s));
@@ -1655,17 +1648,8 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   v.count_dtype = JFX_F32;
   v.out_sum = group_sums_out;
   v.out_count = group_counts_out;
-  ga.slot_gid = bb.g.slot_gid;
-  ga.slot_started = bb.g.slot_started;
-  ga.slot_state = bb.g.slot_state;
-  ga.nslots = 2 * bb.g.nwarps;
-  const unsigned blocks = (unsigned)((bb.g.nwarps * 32 + 255) / 256);
   if (n) {
-    k_group_count<u32><<<blocks, 256, 0, s>>>(ga, bb.g.nwarps), note_launch();
-    JFX_TRY(device_exclusive_scan<u32>(bb.g.warp_count, bb.g.nwarps, bb.g.warp_base, bb.g.total, bb.g.partial, s));
-    JFX_CUDA(cudaMemsetAsync(bb.g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
-    k_group_reduce<u32><<<blocks, 256, 0, s>>>(ga, bb.g.nwarps), note_launch();
-    k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
+    JFX_TRY(launch_group_reduce<u32>(ga, bb.g, (u64)n, s));
   } else {
     JFX_CUDA(cudaMemsetAsync(bb.g.total, 0, sizeof(u32), s));
   }
