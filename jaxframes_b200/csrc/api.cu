@@ -97,6 +97,7 @@ struct GroupBuffers {
   u32* partial;
   u32* total;
   u32* starts;  // [groups + 1] first row of each group
+  u32* big;     // [1 + n / kWarpGroup + 1] groups for k_group_big
   u64 nwarps;
 };
 static void take_group_buffers(Arena& ar, u64 n, GroupBuffers& g) {
@@ -106,6 +107,7 @@ static void take_group_buffers(Arena& ar, u64 n, GroupBuffers& g) {
   g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
   g.total = ar.take<u32>(4);
   g.starts = ar.take<u32>(n + 1);
+  g.big = ar.take<u32>(n / kWarpGroup + 2);
 }
 static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b, GroupBuffers& g) {
   take_common(ar, c);
@@ -126,7 +128,9 @@ static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream
   JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
   k_group_starts<K><<<blocks, 256, 0, s>>>(ga, g.nwarps, g.starts), note_launch();
   k_group_end<<<1, 1, 0, s>>>(g.starts, g.total, n), note_launch();
-  k_group_agg<<<grid_for(n, 256), 256, 0, s>>>(ga, g.starts, g.total), note_launch();
+  JFX_CUDA(cudaMemsetAsync(g.big, 0, sizeof(u32), s));
+  k_group_agg<<<grid_for(n, 256), 256, 0, s>>>(ga, g.starts, g.total, g.big), note_launch();
+  k_group_big<<<device_sm_count() * 4, 256, 0, s>>>(ga, g.starts, g.big), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }

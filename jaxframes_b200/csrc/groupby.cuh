@@ -10,9 +10,8 @@
 // k_group_count counts group starts per warp of 32 * kGroupIPT sorted rows; an
 // exclusive scan of the counts numbers the groups; k_group_starts writes each
 // group's first row and key columns; k_group_agg reduces each group's rows
-// with one thread per group (one warp for a group of more than kSmallGroup
-// rows), so outputs are written by consecutive threads for consecutive
-// groups.  Float sums are accumulated in float64 in row order and rounded
+// with one thread per group (a warp or a CTA for larger groups), so outputs
+// are written by consecutive threads for consecutive groups.  Float sums are accumulated in float64 in row order and rounded
 // once, so results are deterministic.
 #pragma once
 
@@ -302,7 +301,9 @@ __device__ __forceinline__ void agg_finalize(const ValDesc& v, u64 g, const Agg<
 // k_group_agg reduces each group's rows: thread g of the grid owns group g,
 // so every output column is written with consecutive threads on consecutive
 // groups.  A group of more than kSmallGroup rows is reduced by the whole warp
-// instead (lanes fold contiguous shares, then combine in lane order).
+// instead, and one of more than kWarpGroup rows (the heavy keys of a skewed
+// column) by a whole CTA in k_group_big; both read coalesced and combine the
+// rows in row order.
 
 constexpr u32 kSmallGroup = 32;
 
@@ -380,14 +381,9 @@ __device__ __forceinline__ Agg<KIND> agg_rows(const GroupArgs& a, const ValDesc&
   return acc;
 }
 
-// Rows [s, e) folded by the whole warp: lane l takes a contiguous share, the
-// shares combine in lane order; the result is valid in lane 0.
+// Ordered combine of the warp's per-lane states: lane order, result in lane 0.
 template <int KIND>
-__device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 s,
-                                                   u32 e, int lane) {
-  const u32 cnt = e - s, share = (cnt + 31) / 32;
-  const u32 j0 = min(e, s + (u32)lane * share), j1 = min(e, j0 + share);
-  Agg<KIND> acc = agg_rows<KIND>(a, v, need_vals, j0, j1);
+__device__ __forceinline__ Agg<KIND> warp_combine_ordered(Agg<KIND> acc, int lane) {
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     Agg<KIND> up;
@@ -400,13 +396,34 @@ __device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const Val
   return acc;
 }
 
+// Rows [s, e) folded by the whole warp in row order, reading coalesced: each
+// round covers 32 * kWarpRun consecutive rows, lane l folding the kWarpRun
+// rows from s + round + l * kWarpRun; the 32 lane states combine in lane
+// order and the round's state joins the running one.  Valid in lane 0.
+constexpr int kWarpRun = 4;
 template <int KIND>
-__device__ __forceinline__ void agg_column(const GroupArgs& a, int c, bool valid, u32 g, u32 s, u32 e, bool big,
+__device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 s,
+                                                   u32 e, int lane) {
+  Agg<KIND> acc = agg_identity<KIND>();
+  for (u32 r0 = s; r0 < e; r0 += 32 * kWarpRun) {
+    const u32 j0 = min(e, r0 + (u32)lane * kWarpRun), j1 = min(e, j0 + kWarpRun);
+    Agg<KIND> part = warp_combine_ordered<KIND>(agg_rows<KIND>(a, v, need_vals, j0, j1), lane);
+    if (lane == 0) acc = agg_combine<KIND>(acc, part);
+  }
+  return acc;
+}
+
+// Groups of more than kWarpGroup rows are listed by k_group_agg and reduced by
+// k_group_big, one CTA each.
+constexpr u32 kWarpGroup = 8192;
+
+template <int KIND>
+__device__ __forceinline__ void agg_column(const GroupArgs& a, int c, bool valid, u32 g, u32 s, u32 e, bool mid,
                                            int lane) {
   const ValDesc& v = a.v[c];
   const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
-  if (valid && !big) agg_finalize<KIND>(v, g, agg_rows<KIND>(a, v, need_vals, s, e));
-  for (u32 m = __ballot_sync(0xffffffffu, big); m; m &= m - 1) {
+  if (valid && e - s <= kSmallGroup) agg_finalize<KIND>(v, g, agg_rows<KIND>(a, v, need_vals, s, e));
+  for (u32 m = __ballot_sync(0xffffffffu, mid); m; m &= m - 1) {
     const int L = __ffs(m) - 1;
     const u32 gs = __shfl_sync(0xffffffffu, s, L), ge = __shfl_sync(0xffffffffu, e, L);
     const u32 gg = __shfl_sync(0xffffffffu, g, L);
@@ -415,7 +432,8 @@ __device__ __forceinline__ void agg_column(const GroupArgs& a, int c, bool valid
   }
 }
 
-__global__ void __launch_bounds__(256) k_group_agg(GroupArgs a, const u32* starts, const u32* total) {
+// big: [0] count, then group ids (capacity n / kWarpGroup + 1).
+__global__ void __launch_bounds__(256) k_group_agg(GroupArgs a, const u32* starts, const u32* total, u32* big) {
   const u32 G = *total;
   const int lane = threadIdx.x & 31;
   const u64 stride = (u64)gridDim.x * blockDim.x;
@@ -423,12 +441,62 @@ __global__ void __launch_bounds__(256) k_group_agg(GroupArgs a, const u32* start
     const u64 g = g0 + lane;
     const bool valid = g < G;
     const u32 s = valid ? starts[g] : 0u, e = valid ? starts[g + 1] : 0u;
-    const bool big = valid && e - s > kSmallGroup;
+    const bool large = valid && e - s > kWarpGroup;
+    const bool mid = valid && !large && e - s > kSmallGroup;
+    if (large) big[1 + atomicAdd(&big[0], 1u)] = (u32)g;
     for (int c = 0; c < a.nvals; ++c) {
       switch (a.v[c].kind) {
-        case VK_F: agg_column<VK_F>(a, c, valid, (u32)g, s, e, big, lane); break;
-        case VK_I: agg_column<VK_I>(a, c, valid, (u32)g, s, e, big, lane); break;
-        default: agg_column<VK_U>(a, c, valid, (u32)g, s, e, big, lane); break;
+        case VK_F: agg_column<VK_F>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
+        case VK_I: agg_column<VK_I>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
+        default: agg_column<VK_U>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
+      }
+    }
+  }
+}
+
+// One listed group per CTA: warp w folds the w-th contiguous share of the
+// rows (agg_rows_warp), the warps' states combine in warp order.
+template <int KIND>
+__device__ __forceinline__ void big_column(const GroupArgs& a, int c, u32 g, u32 s, u32 e, u64* sh) {
+  const ValDesc& v = a.v[c];
+  const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const u32 share = (e - s + warps - 1) / warps;
+  const u32 j0 = min(e, s + (u32)warp * share), j1 = min(e, j0 + share);
+  const Agg<KIND> r = agg_rows_warp<KIND>(a, v, need_vals, j0, j1, lane);
+  if (lane == 0) {
+    sh[4 * warp] = r.sum;
+    sh[4 * warp + 1] = r.mn;
+    sh[4 * warp + 2] = r.mx;
+    sh[4 * warp + 3] = r.cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Agg<KIND> acc = agg_identity<KIND>();
+    for (int w = 0; w < warps; ++w) {
+      Agg<KIND> x;
+      x.sum = sh[4 * w];
+      x.mn = sh[4 * w + 1];
+      x.mx = sh[4 * w + 2];
+      x.cnt = (u32)sh[4 * w + 3];
+      acc = agg_combine<KIND>(acc, x);
+    }
+    agg_finalize<KIND>(v, g, acc);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_group_big(GroupArgs a, const u32* starts, const u32* big) {
+  __shared__ u64 sh[4 * 32];
+  const u32 count = big[0];
+  for (u32 i = blockIdx.x; i < count; i += gridDim.x) {
+    const u32 g = big[1 + i];
+    const u32 s = starts[g], e = starts[g + 1];
+    for (int c = 0; c < a.nvals; ++c) {
+      switch (a.v[c].kind) {
+        case VK_F: big_column<VK_F>(a, c, g, s, e, sh); break;
+        case VK_I: big_column<VK_I>(a, c, g, s, e, sh); break;
+        default: big_column<VK_U>(a, c, g, s, e, sh); break;
       }
     }
   }

@@ -100,7 +100,25 @@ def join_encoded_strings(left_keys, right_keys, num_codes: int, how: str) -> Str
     ld, rd = _domain(lk, null), _domain(rk, null)
     j = P.ParallelSortMergeJoin()
     neg = lambda k: torch.full((k,), -1, dtype=torch.int32, device=lk.device)
-    if _right_is_unique(rd):
+    rows = lambda k: torch.arange(k, dtype=torch.int32, device=lk.device)
+    unique = _right_is_unique(rd)
+    if ld.numel() == 0 or rd.numel() == 0:
+        # one side empty: nothing matches; the other side's rows are kept by
+        # left / right / outer joins, in row order when the right side is
+        # unique and by code (row order inside a code) otherwise
+        if how == "inner" or (how == "left" and ld.numel() == 0) or (how == "right" and rd.numel() == 0) or \
+                ld.numel() + rd.numel() == 0:
+            e = ld[:0]
+            return StringJoinPlan(e, e.clone(), e.clone())
+        if ld.numel():
+            li, ri, codes = rows(ld.numel()), neg(ld.numel()), ld
+        else:
+            li, ri, codes = neg(rd.numel()), rows(rd.numel()), rd
+        if not unique and ld.numel() == 0:
+            order = _stable_order(codes)
+            codes, ri = _take(codes, order), _take(ri, order)
+        return StringJoinPlan(_restore(codes, null), li, ri)
+    if unique:
         # join_multi_indices emits matches in left row order (one right row
         # each), then the unmatched left rows, then the unmatched right rows
         li, ri = j.join_multi_indices([ld], [rd], how)
