@@ -302,7 +302,7 @@ __device__ __forceinline__ void agg_finalize(const ValDesc& v, u64 g, const Agg<
 // so every output column is written with consecutive threads on consecutive
 // groups.  A group of more than kSmallGroup rows is reduced by the whole warp
 // instead, and one of more than kWarpGroup rows (the heavy keys of a skewed
-// column) by a whole CTA in k_group_big; both read coalesced and combine the
+// column) by a whole CTA in k_group_big, many at once; both read coalesced and combine the
 // rows in row order.
 
 constexpr u32 kSmallGroup = 32;
@@ -400,14 +400,33 @@ __device__ __forceinline__ Agg<KIND> warp_combine_ordered(Agg<KIND> acc, int lan
 // round covers 32 * kWarpRun consecutive rows, lane l folding the kWarpRun
 // rows from s + round + l * kWarpRun; the 32 lane states combine in lane
 // order and the round's state joins the running one.  Valid in lane 0.
-constexpr int kWarpRun = 4;
+// Rows [j0, min(j0 + R, e)) folded in row order, every load issued first.
+template <int KIND, int R>
+__device__ __forceinline__ Agg<KIND> fold_run(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 j0, u32 e) {
+  u64 w[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) w[u] = (need_vals && j0 + u < e) ? row_value<KIND>(a, v, j0 + u) : 0ull;
+  Agg<KIND> part = agg_identity<KIND>();
+#pragma unroll
+  for (int u = 0; u < R; ++u) {
+    if (j0 + u < e) {
+      Agg<KIND> r;
+      r.cnt = 1;
+      r.sum = r.mn = r.mx = w[u];
+      part = agg_combine<KIND>(part, r);
+    }
+  }
+  return part;
+}
+
+constexpr int kWarpRun = 8;
 template <int KIND>
 __device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 s,
                                                    u32 e, int lane) {
   Agg<KIND> acc = agg_identity<KIND>();
   for (u32 r0 = s; r0 < e; r0 += 32 * kWarpRun) {
-    const u32 j0 = min(e, r0 + (u32)lane * kWarpRun), j1 = min(e, j0 + kWarpRun);
-    Agg<KIND> part = warp_combine_ordered<KIND>(agg_rows<KIND>(a, v, need_vals, j0, j1), lane);
+    const u32 j0 = min(e, r0 + (u32)lane * kWarpRun);
+    Agg<KIND> part = warp_combine_ordered<KIND>(fold_run<KIND, kWarpRun>(a, v, need_vals, j0, e), lane);
     if (lane == 0) acc = agg_combine<KIND>(acc, part);
   }
   return acc;
@@ -415,7 +434,7 @@ __device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const Val
 
 // Groups of more than kWarpGroup rows are listed by k_group_agg and reduced by
 // k_group_big, one CTA each.
-constexpr u32 kWarpGroup = 8192;
+constexpr u32 kWarpGroup = 512;
 
 template <int KIND>
 __device__ __forceinline__ void agg_column(const GroupArgs& a, int c, bool valid, u32 g, u32 s, u32 e, bool mid,
@@ -454,36 +473,41 @@ __global__ void __launch_bounds__(256) k_group_agg(GroupArgs a, const u32* start
   }
 }
 
-// One listed group per CTA: warp w folds the w-th contiguous share of the
-// rows (agg_rows_warp), the warps' states combine in warp order.
+// One listed group per CTA, in rounds of kBigRun * blockDim.x consecutive
+// rows: thread t loads rows round + t * kBigRun .. + kBigRun (all loads issued
+// before the first is used) and folds them; the threads' states combine in
+// thread order (warps in lane order, then the warps in order through shared
+// memory) and join the running state in thread 0.
+constexpr int kBigRun = 8;
 template <int KIND>
 __device__ __forceinline__ void big_column(const GroupArgs& a, int c, u32 g, u32 s, u32 e, u64* sh) {
   const ValDesc& v = a.v[c];
   const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  const u32 share = (e - s + warps - 1) / warps;
-  const u32 j0 = min(e, s + (u32)warp * share), j1 = min(e, j0 + share);
-  const Agg<KIND> r = agg_rows_warp<KIND>(a, v, need_vals, j0, j1, lane);
-  if (lane == 0) {
-    sh[4 * warp] = r.sum;
-    sh[4 * warp + 1] = r.mn;
-    sh[4 * warp + 2] = r.mx;
-    sh[4 * warp + 3] = r.cnt;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    Agg<KIND> acc = agg_identity<KIND>();
-    for (int w = 0; w < warps; ++w) {
-      Agg<KIND> x;
-      x.sum = sh[4 * w];
-      x.mn = sh[4 * w + 1];
-      x.mx = sh[4 * w + 2];
-      x.cnt = (u32)sh[4 * w + 3];
-      acc = agg_combine<KIND>(acc, x);
+  Agg<KIND> acc = agg_identity<KIND>();
+  for (u32 r0 = s; r0 < e; r0 += kBigRun * blockDim.x) {
+    const u32 j0 = min(e, r0 + threadIdx.x * kBigRun);
+    Agg<KIND> part = warp_combine_ordered<KIND>(fold_run<KIND, kBigRun>(a, v, need_vals, j0, e), lane);
+    if (lane == 0) {
+      sh[4 * warp] = part.sum;
+      sh[4 * warp + 1] = part.mn;
+      sh[4 * warp + 2] = part.mx;
+      sh[4 * warp + 3] = part.cnt;
     }
-    agg_finalize<KIND>(v, g, acc);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < warps; ++q) {
+        Agg<KIND> x;
+        x.sum = sh[4 * q];
+        x.mn = sh[4 * q + 1];
+        x.mx = sh[4 * q + 2];
+        x.cnt = (u32)sh[4 * q + 3];
+        acc = agg_combine<KIND>(acc, x);
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
+  if (threadIdx.x == 0) agg_finalize<KIND>(v, g, acc);
 }
 
 __global__ void __launch_bounds__(256) k_group_big(GroupArgs a, const u32* starts, const u32* big) {
