@@ -96,18 +96,20 @@ struct GroupBuffers {
   u32* warp_base;
   u32* partial;
   u32* total;
-  u32* starts;  // [groups + 1] first row of each group
-  u32* big;     // [1 + n / kWarpGroup + 1] groups for k_group_big
+  u32* slot_gid;
+  u32* slot_started;
+  u64* slot_state;
   u64 nwarps;
 };
-static void take_group_buffers(Arena& ar, u64 n, GroupBuffers& g) {
+static void take_group_buffers(Arena& ar, u64 n, int nvals, GroupBuffers& g) {
   g.nwarps = (n + 32 * kGroupIPT - 1) / (32 * kGroupIPT);
   g.warp_count = ar.take<u32>(g.nwarps + 1);
   g.warp_base = ar.take<u32>(g.nwarps + 1);
   g.partial = ar.take<u32>(scan_partials_count(g.nwarps));
   g.total = ar.take<u32>(4);
-  g.starts = ar.take<u32>(n + 1);
-  g.big = ar.take<u32>(n / kWarpGroup + 2);
+  g.slot_gid = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_started = ar.take<u32>(2 * g.nwarps + 1);
+  g.slot_state = ar.take<u64>((u64)std::max(nvals, 1) * 4 * (2 * g.nwarps + 1));
 }
 static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b, GroupBuffers& g) {
   take_common(ar, c);
@@ -115,22 +117,26 @@ static void carve_groupby(Arena& ar, u64 n, int nvals, Common& c, SortBuffers& b
   g.sk = ar.take<u64>(n ? n : 1);
   g.perm = ar.take<u32>(n ? n : 1);
   for (int w = 0; w < kMaxWords; ++w) g.words[w] = ar.take<u32>(n ? n : 1);
-  take_group_buffers(ar, n, g);
+  take_group_buffers(ar, n, nvals, g);
 }
 
-// Group boundaries, counts, first rows and key columns, then the
-// group-parallel reduction of every value column (groupby.cuh).  n >= 1.
+// Group boundaries and counts, the scan of the per-warp counts, the
+// lane-sequential segmented reduction and the fix-up of groups that span
+// warps (groupby.cuh).  n >= 1.
 template <typename K>
 static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream_t s) {
+  ga.slot_gid = g.slot_gid;
+  ga.slot_started = g.slot_started;
+  ga.slot_state = g.slot_state;
+  ga.nslots = 2 * g.nwarps;
   const unsigned blocks = (unsigned)((g.nwarps * 32 + 255) / 256);
   k_group_count<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
   JFX_CUDA(cudaGetLastError());
   JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
-  k_group_starts<K><<<blocks, 256, 0, s>>>(ga, g.nwarps, g.starts), note_launch();
-  k_group_end<<<1, 1, 0, s>>>(g.starts, g.total, n), note_launch();
-  JFX_CUDA(cudaMemsetAsync(g.big, 0, sizeof(u32), s));
-  k_group_agg<<<grid_for(n, 256), 256, 0, s>>>(ga, g.starts, g.total, g.big), note_launch();
-  k_group_big<<<device_sm_count() * 4, 256, 0, s>>>(ga, g.starts, g.big), note_launch();
+  JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
+  k_group_reduce<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  JFX_CUDA(cudaGetLastError());
+  k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }
@@ -241,6 +247,12 @@ struct LearnedBuffers {
   u32* starts;  // [buckets + 1]
   u32* large;   // [kBucketLargeMax][2]
   u32* bcounts; // [0] large buckets
+  u32* chunks;  // [cap_chunks][3] min/max chunks of the large buckets
+  u64* mm;      // [kBucketLargeMax][2] their min and max
+  u32* cspans;  // [kBucketLargeMax][2] large buckets for k_bucket_sort_large
+  u64* cmins;
+  u32* cbits;
+  u64 cap_chunks;
   u64* tkeys;   // scratch of the large-bucket sorts
   u32* tids;
   u64 s, nb;
@@ -264,6 +276,12 @@ static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBu
   l.nb = ((4 * n) >> kBucketShift) + 1;  // positions lie in [0, 4n)
   l.starts = ar.take<u32>(l.nb + 1);
   l.large = ar.take<u32>(2 * kBucketLargeMax);
+  l.cap_chunks = n / kLargeChunk + kBucketLargeMax + 1;
+  l.chunks = ar.take<u32>(3 * l.cap_chunks);
+  l.mm = ar.take<u64>(2 * kBucketLargeMax);
+  l.cspans = ar.take<u32>(2 * kBucketLargeMax);
+  l.cmins = ar.take<u64>(kBucketLargeMax);
+  l.cbits = ar.take<u32>(kBucketLargeMax);
   l.bcounts = ar.take<u32>(8);
   l.tkeys = ar.take<u64>(n ? n : 1);
   l.tids = ar.take<u32>(n ? n : 1);
@@ -297,12 +315,15 @@ static int plain_sort_u64(const u64* keys, u64 n, u64* sorted_out, u32* perm_out
 // Stable sort of the rows [0, m) of (keys, ids) by key (one large bucket of
 // the learned sort): the plain radix sort over the rows' key range, the ids
 // carried as the payload, through the scratch arrays and back.
-static int sort_rows_u64(u64* keys, u32* ids, u64 m, u64* tkeys, u32* tids, SortBuffers& b, Common& c,
-                         cudaStream_t s) {
+static int sort_rows_u64(u64* keys, u32* ids, u64 m, u64 kmin, int bits, u64* tkeys, u32* tids, SortBuffers& b,
+                         Common& c, cudaStream_t s) {
   jfx_column col{keys, JFX_U64, 0u};
   KeyPlan kp;
   JFX_TRY(build_pack(&col, 1, 0u, false, kp.pack));
-  JFX_TRY(plan_keys(kp, m, c.mm, s));
+  kp.pack.c[0].tmin = kmin;  // the rows' key range is known
+  kp.pack.c[0].bits = bits;
+  kp.pack.c[0].shift = 0;
+  kp.total_bits = bits;
   if (kp.total_bits == 0) return JFX_OK;  // one key: the rows are in row order already
   RadixRequest rq;
   rq.pack = kp.pack;
@@ -363,7 +384,7 @@ static void carve_batch(Arena& ar, u64 n, u64 nq, Common& c, BatchBuffers& b) {
   b.sk = ar.take<u32>(nn);
   b.sv = ar.take<u32>(nn);
   b.group_q = ar.take<u32>(nn);
-  take_group_buffers(ar, n, b.g);
+  take_group_buffers(ar, n, 1, b.g);
 }
 
 // -------------------------------------------------------------- partition ---
@@ -1426,36 +1447,34 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     rq.keys_out = l.spos;
     JFX_TRY(radix_sort(rq, N, b, c.err, s));
   }
-  // 4. sort inside every bucket
+  // 4. sort inside every bucket: most by k_bucket_sort<8>, those of 2049 to
+  // 4096 rows by k_bucket_sort<16>, which lists the larger ones
   JFX_CUDA(cudaMemsetAsync(l.bcounts, 0, 8 * sizeof(u32), s));
   k_bucket_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(l.spos, N, (u32)l.nb, l.starts), note_launch();
   {
-    static SmemAttr attr;
-    JFX_TRY(ensure_smem(attr, k_bucket_sort, kBucketSmem));
+    static SmemAttr attr8, attr16;
+    JFX_TRY(ensure_smem(attr8, k_bucket_sort<8>, bucket_smem<8>()));
+    JFX_TRY(ensure_smem(attr16, k_bucket_sort<16>, bucket_smem<16>()));
     BucketArgs ba;
     ba.keys = sorted_keys_out;
     ba.ids = (u32*)perm_out;
     ba.starts = l.starts;
     ba.nb = (u32)l.nb;
-    ba.large = l.large;
     ba.counts = l.bcounts;
-    const int grid = (int)std::min<u64>(l.nb, (u64)device_sm_count() * 8);
-    k_bucket_sort<<<grid, kBucketThreads, kBucketSmem, s>>>(ba), note_launch();
-    // buckets of more rows than one CTA holds in shared memory (their count
-    // is read on the device: no synchronisation here)
-    LargeArgs la;
-    la.keys = sorted_keys_out;
-    la.ids = (u32*)perm_out;
-    la.tkeys = l.tkeys;
-    la.tids = l.tids;
-    la.large = l.large;
-    la.counts = l.bcounts;
-    k_bucket_sort_large<<<device_sm_count() * 2, kBucketThreads, 0, s>>>(la), note_launch();
+    ba.large = nullptr;
+    ba.min_rows = 0;
+    const int grid = (int)std::min<u64>(l.nb, (u64)device_sm_count() * 12);
+    k_bucket_sort<8><<<grid, kBucketThreads, bucket_smem<8>(), s>>>(ba), note_launch();
+    ba.large = l.large;
+    ba.min_rows = kBucketSmallCap;
+    k_bucket_sort<16><<<grid, kBucketThreads, bucket_smem<16>(), s>>>(ba), note_launch();
   }
   JFX_CUDA(cudaGetLastError());
   JFX_CUDA(cudaMemcpyAsync(host, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host + 1, l.flags, sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaMemcpyAsync(host + 2, l.bcounts, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  std::vector<u32> spans(2 * (size_t)kBucketLargeMax);
+  JFX_CUDA(cudaMemcpyAsync(spans.data(), l.large, spans.size() * sizeof(u32), cudaMemcpyDeviceToHost, s));
   JFX_CUDA(cudaStreamSynchronize(s));
   JFX_TRY(check_err_word((u32)host[0]));
   const u32 ok = (u32)host[1];
@@ -1471,18 +1490,62 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     return check_err_word((u32)host[0]);
   }
   if (nlarge) {
-    // listed buckets of more than kLargeCtaMax rows (many rows of a few keys
-    // the model puts in one bucket): the multi-CTA stable radix sort of
-    // their rows, one call each
-    std::vector<u32> spans(2 * (size_t)nlarge);
-    JFX_CUDA(cudaMemcpyAsync(spans.data(), l.large, spans.size() * sizeof(u32), cudaMemcpyDeviceToHost, s));
+    // buckets of more than 4096 rows (many rows of a few heavy keys, or a
+    // region the model under-predicts): min and max of each by chunks of
+    // kLargeChunk rows over many CTAs; a bucket of one key is in row order
+    // already; the others are sorted by one CTA each (up to kLargeCtaMax
+    // rows) or by the multi-CTA radix sort over their rows
+    std::vector<u32> chunks;
+    for (u32 r = 0; r < nlarge; ++r)
+      for (u32 c0 = spans[2 * r]; c0 < spans[2 * r + 1]; c0 += kLargeChunk) {
+        chunks.push_back(r);
+        chunks.push_back(c0);
+        chunks.push_back(std::min(spans[2 * r + 1], c0 + kLargeChunk));
+      }
+    const u32 nchunks = (u32)(chunks.size() / 3);
+    if (nchunks > l.cap_chunks) return fail(JFX_ERR_CUDA, "internal: %u min/max chunks exceed %llu", nchunks, l.cap_chunks);
+    JFX_CUDA(cudaMemcpyAsync(l.chunks, chunks.data(), chunks.size() * sizeof(u32), cudaMemcpyHostToDevice, s));
+    k_init_pairs<<<grid_for(nlarge, 256), 256, 0, s>>>(l.mm, nlarge), note_launch();
+    k_large_minmax<<<(unsigned)std::min<u64>(nchunks, (u64)device_sm_count() * 8), 256, 0, s>>>(
+        sorted_keys_out, l.chunks, nchunks, l.mm), note_launch();
+    JFX_CUDA(cudaGetLastError());
+    std::vector<u64> mm(2 * (size_t)nlarge);
+    JFX_CUDA(cudaMemcpyAsync(mm.data(), l.mm, mm.size() * sizeof(u64), cudaMemcpyDeviceToHost, s));
     JFX_CUDA(cudaStreamSynchronize(s));
+    std::vector<u32> cspans, cbits;
+    std::vector<u64> cmins;
     bool any = false;
     for (u32 r = 0; r < nlarge; ++r) {
       const u64 b0 = spans[2 * r], b1 = spans[2 * r + 1];
-      if (b1 - b0 <= kLargeCtaMax) continue;
-      JFX_TRY(sort_rows_u64(sorted_keys_out + b0, (u32*)perm_out + b0, b1 - b0, l.tkeys, l.tids, b, c, s));
+      if (mm[2 * r] == mm[2 * r + 1]) continue;  // one key
+      const int bits = bit_length(mm[2 * r + 1] - mm[2 * r]);
+      if (b1 - b0 <= kLargeCtaMax) {
+        cspans.push_back((u32)b0);
+        cspans.push_back((u32)b1);
+        cmins.push_back(mm[2 * r]);
+        cbits.push_back((u32)bits);
+      } else {
+        JFX_TRY(sort_rows_u64(sorted_keys_out + b0, (u32*)perm_out + b0, b1 - b0, mm[2 * r], bits, l.tkeys, l.tids, b,
+                              c, s));
+      }
       any = true;
+    }
+    if (!cmins.empty()) {
+      JFX_CUDA(cudaMemcpyAsync(l.cspans, cspans.data(), cspans.size() * sizeof(u32), cudaMemcpyHostToDevice, s));
+      JFX_CUDA(cudaMemcpyAsync(l.cmins, cmins.data(), cmins.size() * sizeof(u64), cudaMemcpyHostToDevice, s));
+      JFX_CUDA(cudaMemcpyAsync(l.cbits, cbits.data(), cbits.size() * sizeof(u32), cudaMemcpyHostToDevice, s));
+      LargeArgs la;
+      la.keys = sorted_keys_out;
+      la.ids = (u32*)perm_out;
+      la.tkeys = l.tkeys;
+      la.tids = l.tids;
+      la.spans = l.cspans;
+      la.mins = l.cmins;
+      la.bits = l.cbits;
+      la.count = (u32)cmins.size();
+      k_bucket_sort_large<<<(unsigned)std::min<u64>(cmins.size(), (u64)device_sm_count() * 2), kBucketThreads, 0, s>>>(
+          la), note_launch();
+      JFX_CUDA(cudaGetLastError());
     }
     if (any) {
       JFX_TRY(read_back(c.err, sizeof(u32), host, s));

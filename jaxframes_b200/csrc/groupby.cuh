@@ -1,18 +1,17 @@
 // groupby.cuh -- sort-based groupby: segment-boundary flags over the sorted
-// packed keys, then a segmented reduction of each value column gathered
-// through the sort permutation (or carried through the sort).
+// packed keys, then a warp-level segmented reduction of each value column
+// gathered through the sort permutation.
 //
 // Replaces SortBasedGroupBy.groupby_aggregate (parallel_algorithms.py:733-803,
 // boundary flags :767-770, host group count :772, nonzero/cumsum :773-777,
 // jax.ops.segment_* :626-660) and groupby_aggregate_multi_column (:662-731,
 // _scatter_group_aggregate :1212-1228).
 //
-// k_group_count counts group starts per warp of 32 * kGroupIPT sorted rows; an
-// exclusive scan of the counts numbers the groups; k_group_starts writes each
-// group's first row and key columns; k_group_agg reduces each group's rows
-// with one thread per group (a warp or a CTA for larger groups), so outputs
-// are written by consecutive threads for consecutive groups.  Float sums are accumulated in float64 in row order and rounded
-// once, so results are deterministic.
+// Every warp owns 32*IPT consecutive sorted rows.  A group that starts and
+// ends inside one warp is written by that warp.  A group that crosses a warp
+// boundary leaves one partial record per warp it touches (at most two per
+// warp); k_group_fixup combines those records in row order.  Float sums are
+// accumulated in float64 and rounded once, so results are deterministic.
 #pragma once
 
 #include "radix.cuh"
@@ -21,6 +20,7 @@ namespace jfx {
 
 constexpr int kMaxVals = 16;
 constexpr int kGroupIPT = 8;
+constexpr u32 kEmptySlot = 0xffffffffu;
 
 enum : int { VK_F = 0, VK_I = 1, VK_U = 2 };
 
@@ -51,6 +51,10 @@ struct GroupArgs {
   void* uniq_out[kMaxCols];
   int nvals;
   ValDesc v[kMaxVals];
+  u32* slot_gid;      // [2 * warps]
+  u32* slot_started;  // [2 * warps]
+  u64* slot_state;    // [nvals][4][2 * warps]: sum, min, max, count
+  u64 nslots;
   int values_sorted;  // value columns are already in sorted order (perm unused)
 };
 
@@ -219,6 +223,25 @@ __device__ __forceinline__ Agg<KIND> agg_of(const ValDesc& v, u64 row) {
   return s;
 }
 
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_shfl_up(const Agg<KIND>& s, int o) {
+  Agg<KIND> r;
+  r.sum = __shfl_up_sync(0xffffffffu, s.sum, o);
+  r.mn = __shfl_up_sync(0xffffffffu, s.mn, o);
+  r.mx = __shfl_up_sync(0xffffffffu, s.mx, o);
+  r.cnt = __shfl_up_sync(0xffffffffu, s.cnt, o);
+  return r;
+}
+template <int KIND>
+__device__ __forceinline__ Agg<KIND> agg_shfl(const Agg<KIND>& s, int src) {
+  Agg<KIND> r;
+  r.sum = __shfl_sync(0xffffffffu, s.sum, src);
+  r.mn = __shfl_sync(0xffffffffu, s.mn, src);
+  r.mx = __shfl_sync(0xffffffffu, s.mx, src);
+  r.cnt = __shfl_sync(0xffffffffu, s.cnt, src);
+  return r;
+}
+
 __device__ __forceinline__ void store_float(void* base, int dtype, u64 i, double x) {
   if (dtype == JFX_F32) ((float*)base)[i] = (float)x;
   else ((double*)base)[i] = x;
@@ -295,233 +318,267 @@ __device__ __forceinline__ void agg_finalize(const ValDesc& v, u64 g, const Agg<
   }
 }
 
-// ------------------------------------------------- group-parallel reduce ---
-// After k_group_count and the scan of its per-warp counts, k_group_starts
-// writes every group's first row (and the group's key columns), and
-// k_group_agg reduces each group's rows: thread g of the grid owns group g,
-// so every output column is written with consecutive threads on consecutive
-// groups.  A group of more than kSmallGroup rows is reduced by the whole warp
-// instead, and one of more than kWarpGroup rows (the heavy keys of a skewed
-// column) by a whole CTA in k_group_big, many at once; both read coalesced and combine the
-// rows in row order.
-
-constexpr u32 kSmallGroup = 32;
-
-template <typename K>
-__global__ void __launch_bounds__(256) k_group_starts(GroupArgs a, u64 nwarps, u32* starts) {
-  const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nwarps) return;
-  const K* sk = (const K*)a.skeys;
-  const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
-  const u32 lt = lanemask_lt();
-  u32 gbase = a.warp_base[w];
-  K kv[kGroupIPT];
-#pragma unroll
-  for (int q = 0; q < kGroupIPT; ++q) {
-    const u64 row = wbeg + (u64)q * 32 + lane;
-    kv[q] = row < wend ? sk[row] : (K)0;
+template <int KIND>
+__device__ __forceinline__ void slot_store(const GroupArgs& a, int c, u64 slot, u32 gid, u32 started,
+                                           const Agg<KIND>& s) {
+  u64* st = a.slot_state + (u64)c * 4 * a.nslots;
+  st[slot] = s.sum;
+  st[a.nslots + slot] = s.mn;
+  st[2 * a.nslots + slot] = s.mx;
+  st[3 * a.nslots + slot] = s.cnt;
+  if (c == 0) {
+    a.slot_gid[slot] = gid;
+    a.slot_started[slot] = started;
   }
-  K carry = wbeg > 0 ? sk[wbeg - 1] : (K)0;  // the row before this step's first row
+}
+
+// The value of sorted row `pos` (carried columns: lo/hi words already read).
+template <int KIND>
+__device__ __forceinline__ u64 carried_word(const ValDesc& v, u32 lo, u32 hi) {
+  if (dtype_size(v.dtype) == 8) return (u64)lo | ((u64)hi << 32);
+  if (KIND == VK_F) return __double_as_longlong((double)__uint_as_float(lo));
+  if (KIND == VK_I) return (u64)(long long)(int)lo;
+  return (u64)lo;
+}
+
+// One value column over the warp's rows, lane-sequential: lane l owns the
+// kGroupIPT consecutive rows r0.. (bit j of fl: row r0+j starts a group).
+// Pass 1 folds each lane's rows after its last group start; a segmented
+// scan across the 32 lanes gives every lane the part of its first group that
+// lies in earlier lanes; pass 2 walks the lane's rows again and writes each
+// group where it ends.  Groups that begin in an earlier warp or run past the
+// warp end leave slot records for k_group_fixup, as before.
+template <int KIND>
+__device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u64 w, u64 r0, int nv, u32 fl,
+                                                   u32 gfirst, bool last_lane, bool end_closes, bool next_flag,
+                                                   const u32 (&pr)[kGroupIPT]) {
+  const ValDesc& v = a.v[c];
+  const int lane = threadIdx.x & 31;
+  const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
+  u64 word[kGroupIPT];
+  if (need_vals) {
+    if (v.carried) {
+      u32 lo[kGroupIPT], hi[kGroupIPT];
+      const bool wide = dtype_size(v.dtype) == 8;
+      if (nv == kGroupIPT) {
 #pragma unroll
-  for (int q = 0; q < kGroupIPT; ++q) {
-    const u64 row = wbeg + (u64)q * 32 + lane;
-    K kp = __shfl_up_sync(0xffffffffu, kv[q], 1);
-    if (lane == 0) kp = carry;
-    carry = __shfl_sync(0xffffffffu, kv[q], 31);
-    const bool f = row < wend && (row == 0 || kv[q] != kp || packed_has_nan<K>(a.pack, kv[q]));
-    const u32 bal = __ballot_sync(0xffffffffu, f);
-    if (f) {
-      const u32 gid = gbase + __popc(bal & lt);
-      starts[gid] = (u32)row;
-      for (int jc = 0; jc < a.pack.ncols; ++jc) {
-        const ColDesc& cd = a.pack.c[jc];
-        if (!a.uniq_out[jc]) continue;
-        if (dtype_is_float(cd.dtype)) {
-          // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
-          const u32 krow = a.perm ? a.perm[row] : (u32)row;
-          store_raw(a.uniq_out[jc], cd.dtype, gid, load_raw(cd.ptr, cd.dtype, krow));
-        } else {
-          const u64 field =
-              cd.bits ? (((u64)kv[q] >> cd.shift) & (cd.bits >= 64 ? ~0ull : ((1ull << cd.bits) - 1ull))) : 0ull;
-          store_raw(a.uniq_out[jc], cd.dtype, gid, untransform_int(cd.dtype, cd.flags, field + cd.tmin));
+        for (int q = 0; q < kGroupIPT / 4; ++q) {
+          reinterpret_cast<uint4*>(lo)[q] = __ldg(reinterpret_cast<const uint4*>((const u32*)v.ptr + r0) + q);
+          if (wide) reinterpret_cast<uint4*>(hi)[q] = __ldg(reinterpret_cast<const uint4*>((const u32*)v.ptr_hi + r0) + q);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < kGroupIPT; ++j) {
+          lo[j] = j < nv ? __ldg((const u32*)v.ptr + r0 + j) : 0u;
+          hi[j] = (wide && j < nv) ? __ldg((const u32*)v.ptr_hi + r0 + j) : 0u;
         }
       }
+#pragma unroll
+      for (int j = 0; j < kGroupIPT; ++j) word[j] = carried_word<KIND>(v, lo[j], wide ? hi[j] : 0u);
+    } else {
+#pragma unroll
+      for (int j = 0; j < kGroupIPT; ++j) word[j] = j < nv ? value_word<KIND>(v, pr[j]) : 0ull;
     }
-    gbase += __popc(bal);
+  }
+  // pass 1: the lane's rows after its last group start (all rows without one)
+  Agg<KIND> tail = agg_identity<KIND>();
+#pragma unroll
+  for (int j = 0; j < kGroupIPT; ++j) {
+    if (j >= nv) break;
+    if ((fl >> j) & 1u) tail = agg_identity<KIND>();
+    Agg<KIND> r;
+    r.cnt = 1;
+    r.sum = r.mn = r.mx = need_vals ? word[j] : 0ull;
+    tail = agg_combine<KIND>(tail, r);
+  }
+  // segmented inclusive scan over lanes: a lane with a group start restarts
+  Agg<KIND> run = tail;
+  bool seg = fl != 0u;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const Agg<KIND> up = agg_shfl_up<KIND>(run, o);
+    const bool useg = __shfl_up_sync(0xffffffffu, seg, o);
+    if (lane >= o && !seg) {
+      run = agg_combine<KIND>(up, run);
+      seg = useg;
+    }
+  }
+  // the part of the lane's first group in earlier lanes, and whether that
+  // group began inside this warp
+  Agg<KIND> cur = agg_shfl_up<KIND>(run, 1);
+  bool cur_started = __shfl_up_sync(0xffffffffu, seg, 1);
+  bool cur_rows = lane > 0;
+  if (lane == 0) {
+    cur = agg_identity<KIND>();
+    cur_started = false;
+  }
+  u32 cur_gid = gfirst - 1u;
+  // pass 2: write every group that ends inside the lane
+#pragma unroll 1
+  for (int j = 0; j < nv; ++j) {
+    if ((fl >> j) & 1u) {
+      if (cur_rows) {
+        if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
+        else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);  // the warp's first group, begun earlier
+      }
+      cur = agg_identity<KIND>();
+      cur_started = true;
+      cur_gid = gfirst + __popc(fl & ((1u << j) - 1u));
+    }
+    Agg<KIND> r;
+    r.cnt = 1;
+    r.sum = r.mn = r.mx = need_vals ? word[j] : 0ull;
+    cur = agg_combine<KIND>(cur, r);
+    cur_rows = true;
+  }
+  if (nv == 0) return;
+  // the group open at the lane end ends here if the next lane starts a group,
+  // or at the warp end when the row after the warp starts one
+  if (last_lane ? end_closes : next_flag) {
+    if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
+    else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);
+  } else if (last_lane) {
+    slot_store<KIND>(a, c, 2 * w + 1, cur_gid, cur_started ? 1u : 0u, cur);  // open past the warp end
   }
 }
 
-// starts[G] = n: the end of the last group (G read on the device).
-__global__ void k_group_end(u32* starts, const u32* total, u64 n) { starts[*total] = (u32)n; }
-
-template <int KIND>
-__device__ __forceinline__ u64 row_value(const GroupArgs& a, const ValDesc& v, u64 row) {
-  return value_word<KIND>(v, a.values_sorted ? row : (u64)a.perm[row]);
-}
-
-// Rows [s, e) folded in row order by one thread.
-template <int KIND>
-__device__ __forceinline__ Agg<KIND> agg_rows(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 s, u32 e) {
-  Agg<KIND> acc = agg_identity<KIND>();
-  constexpr int U = 4;  // loads issued together
-  for (u32 r0 = s; r0 < e; r0 += U) {
-    u64 w[U];
+template <typename K>
+__global__ void __launch_bounds__(256, 4) k_group_reduce(GroupArgs a, u64 nwarps) {  // 4 CTAs per SM
+  const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nwarps) return;  // whole warps exit together
+  const K* sk = (const K*)a.skeys;
+  const u64 wbeg = w * 32 * kGroupIPT, wend = min(a.n, wbeg + 32 * kGroupIPT);
+  const u64 r0 = wbeg + (u64)lane * kGroupIPT;
+  const int nv = r0 >= wend ? 0 : (int)min((u64)kGroupIPT, wend - r0);
+  K kv[kGroupIPT];
+  if (nv == kGroupIPT && (kGroupIPT * sizeof(K)) % 16 == 0) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) w[u] = (need_vals && r0 + u < e) ? row_value<KIND>(a, v, r0 + u) : 0ull;
+    for (int q = 0; q < kGroupIPT * (int)sizeof(K) / 16; ++q)
+      reinterpret_cast<uint4*>(kv)[q] = __ldg(reinterpret_cast<const uint4*>(sk + r0) + q);
+  } else {
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (r0 + u >= e) break;
-      Agg<KIND> r;
-      r.cnt = 1;
-      r.sum = r.mn = r.mx = w[u];
-      acc = agg_combine<KIND>(acc, r);
+    for (int j = 0; j < kGroupIPT; ++j) kv[j] = j < nv ? sk[r0 + j] : (K)0;
+  }
+  u32 pr[kGroupIPT];
+  if (!a.values_sorted) {
+#pragma unroll
+    for (int j = 0; j < kGroupIPT; ++j) pr[j] = j < nv ? a.perm[r0 + j] : 0u;
+  } else {
+#pragma unroll
+    for (int j = 0; j < kGroupIPT; ++j) pr[j] = (u32)(r0 + j);
+  }
+  // group starts: the key differs from the previous row's (a NaN key is a group of its own)
+  K prev = __shfl_up_sync(0xffffffffu, kv[kGroupIPT - 1], 1);
+  if (lane == 0) prev = wbeg > 0 ? sk[wbeg - 1] : (K)0;
+  u32 fl = 0;
+#pragma unroll
+  for (int j = 0; j < kGroupIPT; ++j) {
+    const K kp = j ? kv[j - 1] : prev;
+    const bool f = j < nv && (r0 + j == 0 || kv[j] != kp || packed_has_nan<K>(a.pack, kv[j]));
+    fl |= (u32)f << j;
+  }
+  // group id of the lane's first start: warp base + starts in earlier lanes
+  const u32 cnt = __popc(fl);
+  u32 inc = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const u32 gfirst = a.warp_base[w] + inc - cnt;
+  // unique key columns of every group starting in the lane
+  for (u32 m = fl; m; m &= m - 1) {
+    const int j = __ffs(m) - 1;
+    const u32 gid = gfirst + __popc(fl & ((1u << j) - 1u));
+    const u64 row = r0 + j;
+    for (int jc = 0; jc < a.pack.ncols; ++jc) {
+      const ColDesc& cd = a.pack.c[jc];
+      if (!a.uniq_out[jc]) continue;
+      if (dtype_is_float(cd.dtype)) {
+        // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
+        const u32 krow = a.perm ? a.perm[row] : (u32)row;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, load_raw(cd.ptr, cd.dtype, krow));
+      } else {
+        const u64 field = cd.bits ? (((u64)kv[j] >> cd.shift) & (cd.bits >= 64 ? ~0ull : ((1ull << cd.bits) - 1ull))) : 0ull;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, untransform_int(cd.dtype, cd.flags, field + cd.tmin));
+      }
     }
   }
-  return acc;
+  const int last = (int)((wend - 1 - wbeg) / kGroupIPT);  // lane holding the warp's last row
+  const bool end_closes = wend < a.n ? row_flag<K>(a, sk, wend) : true;
+  const bool next_flag = __shfl_down_sync(0xffffffffu, fl & 1u, 1) != 0u;
+  for (int c = 0; c < a.nvals; ++c) {
+    switch (a.v[c].kind) {
+      case VK_F: reduce_lane_column<VK_F>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      case VK_I: reduce_lane_column<VK_I>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      default: reduce_lane_column<VK_U>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+    }
+  }
 }
 
-// Ordered combine of the warp's per-lane states: lane order, result in lane 0.
 template <int KIND>
-__device__ __forceinline__ Agg<KIND> warp_combine_ordered(Agg<KIND> acc, int lane) {
+__device__ __forceinline__ Agg<KIND> slot_load(const GroupArgs& a, int c, u64 i) {
+  const u64* st = a.slot_state + (u64)c * 4 * a.nslots;
+  Agg<KIND> s;
+  s.sum = st[i];
+  s.mn = st[a.nslots + i];
+  s.mx = st[2 * a.nslots + i];
+  s.cnt = (u32)st[3 * a.nslots + i];
+  return s;
+}
+
+// The records [i, end) of group g (empty records skipped), combined in row
+// order by one warp: lane l folds a contiguous share of the records, then a
+// tree in lane order joins the shares, so a group spanning many warps costs
+// its record count / 32 steps, not one step per record.
+template <int KIND>
+__device__ void fixup_column(const GroupArgs& a, int c, u64 i, u64 end, u32 g, int lane) {
+  const u64 cnt = end - i, share = (cnt + 31) / 32;
+  const u64 j0 = i + (u64)lane * share, j1 = min(end, j0 + share);
+  Agg<KIND> s = agg_identity<KIND>();
+  for (u64 j = j0; j < j1; ++j)
+    if (a.slot_gid[j] == g) s = agg_combine<KIND>(s, slot_load<KIND>(a, c, j));
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     Agg<KIND> up;
-    up.sum = __shfl_down_sync(0xffffffffu, acc.sum, o);
-    up.mn = __shfl_down_sync(0xffffffffu, acc.mn, o);
-    up.mx = __shfl_down_sync(0xffffffffu, acc.mx, o);
-    up.cnt = __shfl_down_sync(0xffffffffu, acc.cnt, o);
-    if ((lane & (2 * o - 1)) == 0 && lane + o < 32) acc = agg_combine<KIND>(acc, up);
+    up.sum = __shfl_down_sync(0xffffffffu, s.sum, o);
+    up.mn = __shfl_down_sync(0xffffffffu, s.mn, o);
+    up.mx = __shfl_down_sync(0xffffffffu, s.mx, o);
+    up.cnt = __shfl_down_sync(0xffffffffu, s.cnt, o);
+    if ((lane & (2 * o - 1)) == 0 && lane + o < 32) s = agg_combine<KIND>(s, up);
   }
-  return acc;
+  if (lane == 0) agg_finalize<KIND>(a.v[c], g, s);
 }
 
-// Rows [s, e) folded by the whole warp in row order, reading coalesced: each
-// round covers 32 * kWarpRun consecutive rows, lane l folding the kWarpRun
-// rows from s + round + l * kWarpRun; the 32 lane states combine in lane
-// order and the round's state joins the running one.  Valid in lane 0.
-// Rows [j0, min(j0 + R, e)) folded in row order, every load issued first.
-template <int KIND, int R>
-__device__ __forceinline__ Agg<KIND> fold_run(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 j0, u32 e) {
-  u64 w[R];
-#pragma unroll
-  for (int u = 0; u < R; ++u) w[u] = (need_vals && j0 + u < e) ? row_value<KIND>(a, v, j0 + u) : 0ull;
-  Agg<KIND> part = agg_identity<KIND>();
-#pragma unroll
-  for (int u = 0; u < R; ++u) {
-    if (j0 + u < e) {
-      Agg<KIND> r;
-      r.cnt = 1;
-      r.sum = r.mn = r.mx = w[u];
-      part = agg_combine<KIND>(part, r);
-    }
-  }
-  return part;
-}
-
-constexpr int kWarpRun = 8;
-template <int KIND>
-__device__ __forceinline__ Agg<KIND> agg_rows_warp(const GroupArgs& a, const ValDesc& v, bool need_vals, u32 s,
-                                                   u32 e, int lane) {
-  Agg<KIND> acc = agg_identity<KIND>();
-  for (u32 r0 = s; r0 < e; r0 += 32 * kWarpRun) {
-    const u32 j0 = min(e, r0 + (u32)lane * kWarpRun);
-    Agg<KIND> part = warp_combine_ordered<KIND>(fold_run<KIND, kWarpRun>(a, v, need_vals, j0, e), lane);
-    if (lane == 0) acc = agg_combine<KIND>(acc, part);
-  }
-  return acc;
-}
-
-// Groups of more than kWarpGroup rows are listed by k_group_agg and reduced by
-// k_group_big, one CTA each.
-constexpr u32 kWarpGroup = 512;
-
-template <int KIND>
-__device__ __forceinline__ void agg_column(const GroupArgs& a, int c, bool valid, u32 g, u32 s, u32 e, bool mid,
-                                           int lane) {
-  const ValDesc& v = a.v[c];
-  const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
-  if (valid && e - s <= kSmallGroup) agg_finalize<KIND>(v, g, agg_rows<KIND>(a, v, need_vals, s, e));
-  for (u32 m = __ballot_sync(0xffffffffu, mid); m; m &= m - 1) {
-    const int L = __ffs(m) - 1;
-    const u32 gs = __shfl_sync(0xffffffffu, s, L), ge = __shfl_sync(0xffffffffu, e, L);
-    const u32 gg = __shfl_sync(0xffffffffu, g, L);
-    const Agg<KIND> r = agg_rows_warp<KIND>(a, v, need_vals, gs, ge, lane);
-    if (lane == 0) agg_finalize<KIND>(v, gg, r);
-  }
-}
-
-// big: [0] count, then group ids (capacity n / kWarpGroup + 1).
-__global__ void __launch_bounds__(256) k_group_agg(GroupArgs a, const u32* starts, const u32* total, u32* big) {
-  const u32 G = *total;
+// One warp per partial record; the warp of the record holding the group's
+// first row finds the group's following records (same group id, not a group
+// start; empty records in between) 32 at a time and combines them.
+__global__ void __launch_bounds__(256) k_group_fixup(GroupArgs a) {
+  const u64 i = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  const u64 stride = (u64)gridDim.x * blockDim.x;
-  for (u64 g0 = (u64)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); g0 < G; g0 += stride) {
-    const u64 g = g0 + lane;
-    const bool valid = g < G;
-    const u32 s = valid ? starts[g] : 0u, e = valid ? starts[g + 1] : 0u;
-    const bool large = valid && e - s > kWarpGroup;
-    const bool mid = valid && !large && e - s > kSmallGroup;
-    if (large) big[1 + atomicAdd(&big[0], 1u)] = (u32)g;
-    for (int c = 0; c < a.nvals; ++c) {
-      switch (a.v[c].kind) {
-        case VK_F: agg_column<VK_F>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
-        case VK_I: agg_column<VK_I>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
-        default: agg_column<VK_U>(a, c, valid && !large, (u32)g, s, e, mid, lane); break;
-      }
+  if (i >= a.nslots) return;  // whole warps
+  const u32 g = a.slot_gid[i];
+  if (g == kEmptySlot || !a.slot_started[i]) return;
+  u64 end = a.nslots;
+  for (u64 b = i + 1; b < a.nslots; b += 32) {
+    const u64 j = b + lane;
+    bool stop = j >= a.nslots;
+    if (!stop) {
+      const u32 gj = a.slot_gid[j];
+      stop = gj != kEmptySlot && (gj != g || a.slot_started[j]);
+    }
+    const u32 sm = __ballot_sync(0xffffffffu, stop);
+    if (sm) {
+      end = b + __ffs(sm) - 1;
+      break;
     }
   }
-}
-
-// One listed group per CTA, in rounds of kBigRun * blockDim.x consecutive
-// rows: thread t loads rows round + t * kBigRun .. + kBigRun (all loads issued
-// before the first is used) and folds them; the threads' states combine in
-// thread order (warps in lane order, then the warps in order through shared
-// memory) and join the running state in thread 0.
-constexpr int kBigRun = 8;
-template <int KIND>
-__device__ __forceinline__ void big_column(const GroupArgs& a, int c, u32 g, u32 s, u32 e, u64* sh) {
-  const ValDesc& v = a.v[c];
-  const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  Agg<KIND> acc = agg_identity<KIND>();
-  for (u32 r0 = s; r0 < e; r0 += kBigRun * blockDim.x) {
-    const u32 j0 = min(e, r0 + threadIdx.x * kBigRun);
-    Agg<KIND> part = warp_combine_ordered<KIND>(fold_run<KIND, kBigRun>(a, v, need_vals, j0, e), lane);
-    if (lane == 0) {
-      sh[4 * warp] = part.sum;
-      sh[4 * warp + 1] = part.mn;
-      sh[4 * warp + 2] = part.mx;
-      sh[4 * warp + 3] = part.cnt;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int q = 0; q < warps; ++q) {
-        Agg<KIND> x;
-        x.sum = sh[4 * q];
-        x.mn = sh[4 * q + 1];
-        x.mx = sh[4 * q + 2];
-        x.cnt = (u32)sh[4 * q + 3];
-        acc = agg_combine<KIND>(acc, x);
-      }
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) agg_finalize<KIND>(v, g, acc);
-}
-
-__global__ void __launch_bounds__(256) k_group_big(GroupArgs a, const u32* starts, const u32* big) {
-  __shared__ u64 sh[4 * 32];
-  const u32 count = big[0];
-  for (u32 i = blockIdx.x; i < count; i += gridDim.x) {
-    const u32 g = big[1 + i];
-    const u32 s = starts[g], e = starts[g + 1];
-    for (int c = 0; c < a.nvals; ++c) {
-      switch (a.v[c].kind) {
-        case VK_F: big_column<VK_F>(a, c, g, s, e, sh); break;
-        case VK_I: big_column<VK_I>(a, c, g, s, e, sh); break;
-        default: big_column<VK_U>(a, c, g, s, e, sh); break;
-      }
+  for (int c = 0; c < a.nvals; ++c) {
+    switch (a.v[c].kind) {
+      case VK_F: fixup_column<VK_F>(a, c, i, end, g, lane); break;
+      case VK_I: fixup_column<VK_I>(a, c, i, end, g, lane); break;
+      default: fixup_column<VK_U>(a, c, i, end, g, lane); break;
     }
   }
 }

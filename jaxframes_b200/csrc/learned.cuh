@@ -196,8 +196,10 @@ __global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n,
 constexpr int kBucketShift = 13;  // positions in [0, 4n): 8192 positions, about 2048 rows, per bucket
 constexpr int kBucketThreads = 256, kBucketIPT = 16;
 constexpr u32 kBucketCap = kBucketThreads * kBucketIPT;  // rows one CTA sorts in shared memory
+constexpr u32 kBucketSmallCap = kBucketThreads * 8;       // buckets the 8-item instantiation takes
 constexpr u32 kBucketLargeMax = 4096;                     // large buckets listed per call
 constexpr u32 kLargeCtaMax = 1u << 20;  // larger buckets: the multi-CTA radix sort, one call each
+constexpr u32 kLargeChunk = 1u << 16;   // rows per CTA of the large buckets' min/max
 
 // starts[c] = first row of bucket c in the bucket-sorted ids sb[0..n), for
 // c in [0, nb]; an empty bucket starts where the next non-empty one does.
@@ -214,8 +216,10 @@ struct BucketArgs {
   u32* ids;            // in/out: their row ids
   const u32* starts;   // [nb + 1]
   u32 nb;
-  u32* large;          // [kBucketLargeMax][2] buckets of more than kBucketCap rows: (start, end)
+  u32* large;          // [kBucketLargeMax][2] buckets of more than kBucketCap rows: (start, end),
+                       // or null: such buckets are left to another launch
   u32* counts;         // [0] large buckets found
+  u32 min_rows;        // buckets of at most this many rows are left to another launch
 };
 
 // Min and max key of rows [s, e), by the whole CTA (red: 2 * warps words).
@@ -248,19 +252,26 @@ __device__ __forceinline__ void block_minmax(const u64* keys, u32 s, u32 e, u64*
   __syncthreads();
 }
 
-constexpr size_t kBucketSmem = (size_t)kBucketCap * (8 + 4) + (size_t)2 * 8 * 256 * 4 + 256 * 4 + 32 * 4 + 16 * 8;
+template <int IPT>
+constexpr size_t bucket_smem() {
+  return (size_t)kBucketThreads * IPT * (8 + 4) + (size_t)2 * 8 * 256 * 4 + 256 * 4 + 32 * 4 + 16 * 8;
+}
 
 // One bucket at a time per CTA: a stable LSD radix sort of key - min in
 // shared memory over bit_length(max - min) bits, 8 bits per pass.  Warp w
 // owns the bucket's rows [w * seg, (w + 1) * seg), seg = ceil(m / 8); item i
 // of lane l is row w * seg + 32 i + l, so (warp, item, lane) order is row
 // order and the warp ranking keeps equal digits in row order.
-__global__ void __launch_bounds__(kBucketThreads, 2) k_bucket_sort(BucketArgs a) {
-  constexpr int IPT = kBucketIPT, RADIX = 256, WARPS = kBucketThreads / 32;
+// IPT = 8 takes buckets of min_rows + 1 .. 2048 rows (most buckets, in fewer
+// registers); IPT = 16 takes 2049 .. 4096 rows and lists the larger ones.
+template <int IPT>
+__global__ void __launch_bounds__(kBucketThreads, IPT <= 8 ? 3 : 2) k_bucket_sort(BucketArgs a) {
+  constexpr int RADIX = 256, WARPS = kBucketThreads / 32;
+  constexpr u32 CAP = (u32)kBucketThreads * IPT;
   extern __shared__ __align__(16) unsigned char smem[];
-  u64* skeys = (u64*)smem;                       // [kBucketCap]
-  u32* sids = (u32*)(skeys + kBucketCap);        // [kBucketCap]
-  u32* whist = sids + kBucketCap;                // [WARPS][RADIX] counters
+  u64* skeys = (u64*)smem;                       // [CAP]
+  u32* sids = (u32*)(skeys + CAP);               // [CAP]
+  u32* whist = sids + CAP;                       // [WARPS][RADIX] counters
   u32* wmask = whist + WARPS * RADIX;            // [WARPS][RADIX] peer masks
   u32* sexcl = wmask + WARPS * RADIX;            // [RADIX]
   u32* sscan = sexcl + RADIX;                    // [32]
@@ -269,9 +280,9 @@ __global__ void __launch_bounds__(kBucketThreads, 2) k_bucket_sort(BucketArgs a)
   for (int i = tid; i < WARPS * RADIX; i += kBucketThreads) wmask[i] = 0u;
   for (u32 b = blockIdx.x; b < a.nb; b += gridDim.x) {
     const u32 s = a.starts[b], e = a.starts[b + 1], m = e - s;
-    if (m <= 1) continue;
-    if (m > kBucketCap) {  // listed for k_bucket_sort_large or the host
-      if (tid == 0) {
+    if (m <= 1 || m <= a.min_rows) continue;
+    if (m > CAP) {  // listed for k_bucket_sort_large or the host
+      if (a.large && tid == 0) {
         const u32 r = atomicAdd(&a.counts[0], 1u);
         if (r < kBucketLargeMax) {
           a.large[2 * r] = s;
@@ -376,32 +387,53 @@ struct LargeArgs {
   u32* ids;
   u64* tkeys;          // scratch, same positions
   u32* tids;
-  const u32* large;    // [count][2] (start, end)
-  const u32* counts;   // [0] listed buckets (at most kBucketLargeMax are in the list)
+  const u32* spans;    // [count][2] (start, end) of buckets holding more than one key
+  const u64* mins;     // [count] their smallest key
+  const u32* bits;     // [count] bit_length(max - min)
+  u32 count;
 };
 
-// Listed large buckets of at most kLargeCtaMax rows, one CTA each: min and
-// max of the bucket's keys, then a stable LSD radix sort of key - min, 8 bits
-// per pass, through the scratch arrays (a bucket of one key is left as is).
-// Per pass a counting read gives each digit's first position; then chunks of
-// kBucketCap rows in row order are ranked as in k_bucket_sort (warp w owns
-// rows [512 w, 512 w + 512) of the chunk) and written to the digit's next
-// positions, so equal digits keep row order across chunks.
+// Min and max key of every listed large bucket: one CTA per chunk of
+// kLargeChunk rows (chunks: [r, start, end] triples), atomics into mm[2r],
+// mm[2r + 1] (set to ~0 / 0 beforehand).
+__global__ void __launch_bounds__(256) k_large_minmax(const u64* keys, const u32* chunks, u32 nchunks, u64* mm) {
+  __shared__ u64 red[16];
+  for (u32 c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const u32 r = chunks[3 * c], s = chunks[3 * c + 1], e = chunks[3 * c + 2];
+    u64 mn, mx;
+    block_minmax(keys, s, e, red, mn, mx);
+    if (threadIdx.x == 0) {
+      atomicMin(&mm[2 * r], mn);
+      atomicMax(&mm[2 * r + 1], mx);
+    }
+  }
+}
+
+__global__ void k_init_pairs(u64* mm, u32 count) {
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    mm[2 * i] = ~0ull;
+    mm[2 * i + 1] = 0ull;
+  }
+}
+
+// The large buckets of at most kLargeCtaMax rows that hold more than one key,
+// one CTA each: a stable LSD radix sort of key - min, 8 bits per pass,
+// through the scratch arrays.  Per pass a counting read gives each digit's
+// first position; then chunks of kBucketCap rows in row order are ranked as
+// in k_bucket_sort (warp w owns rows [512 w, 512 w + 512) of the chunk) and
+// written to the digit's next positions, so equal digits keep row order
+// across chunks.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(LargeArgs a) {
   constexpr int IPT = kBucketIPT, RADIX = 256, WARPS = kBucketThreads / 32, SEG = 32 * IPT;
   __shared__ u32 whist[WARPS * RADIX];
   __shared__ u32 wmask[WARPS * RADIX];
   __shared__ u32 sbase[RADIX], stot[RADIX], sscan[32];
-  __shared__ u64 sred[2 * WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < WARPS * RADIX; i += kBucketThreads) wmask[i] = 0u;
-  const u32 count = min(a.counts[0], kBucketLargeMax);
-  for (u32 r = blockIdx.x; r < count; r += gridDim.x) {
-    const u32 s = a.large[2 * r], e = a.large[2 * r + 1];
-    if (e - s > kLargeCtaMax) continue;  // the host sorts it
-    u64 mn, mx;
-    block_minmax(a.keys, s, e, sred, mn, mx);
-    const int bits = bit_length(mx - mn);  // 0: one key, the rows are in row order already
+  for (u32 r = blockIdx.x; r < a.count; r += gridDim.x) {
+    const u32 s = a.spans[2 * r], e = a.spans[2 * r + 1];
+    const u64 mn = a.mins[r];
+    const int bits = (int)a.bits[r];
     u64* ks = a.keys;
     u32* is = a.ids;
     u64* kd = a.tkeys;

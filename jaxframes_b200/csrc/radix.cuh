@@ -106,6 +106,60 @@ __device__ __forceinline__ void warp_rank_or(u32 (&rd)[IPT], u32* wh, u32* wm, i
   }
 }
 
+// The same ranking with every other item ranked by ballots instead of the
+// shared-memory masks (one ballot per digit bit, the highest peer advances
+// the counter with a shared-memory atomic): the mask ranking loads the
+// shared-memory pipe and the ballot ranking the integer pipe, and in a radix
+// pass whose shared-memory traffic is already high, splitting the items
+// between the two keeps either from saturating.  Same counters, same output.
+template <int IPT, int RADIX, int RB>
+__device__ __forceinline__ void warp_rank_mixed(u32 (&rd)[IPT], u32* wh, u32* wm, int lane) {
+  const u32 lt = lanemask_lt(), bit = 1u << lane;
+#pragma unroll
+  for (int i = 0; i < IPT; ++i) {
+    const u32 d = rd[i];
+    const bool valid = d < (u32)RADIX;
+    u32 rank;
+    if (i & 1) {
+      u32 peers = __ballot_sync(0xffffffffu, valid);
+      if (!valid) peers = ~peers;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) {
+        const u32 db = (d >> b) & 1u;
+        const u32 bb = __ballot_sync(0xffffffffu, db);
+        peers &= db ? bb : ~bb;
+      }
+      const int leader = 31 - __clz(peers);
+      u32 prior = 0;
+      if (valid && lane == leader) prior = atomicAdd(&wh[d], (u32)__popc(peers));
+      prior = __shfl_sync(0xffffffffu, prior, leader);
+      rank = prior + (u32)__popc(peers & lt);
+      __syncwarp();
+    } else {
+      const u32 d0 = __shfl_sync(0xffffffffu, d, 0);
+      if (__all_sync(0xffffffffu, d == d0)) {
+        const u32 before = valid ? wh[d] : 0u;
+        __syncwarp();
+        if (valid && lane == 31) wh[d] = before + 32u;
+        rank = before + (u32)lane;
+      } else {
+        if (valid) atomicOr(&wm[d], bit);
+        __syncwarp();
+        const u32 peers = valid ? wm[d] : 0u;
+        const u32 before = valid ? wh[d] : 0u;
+        __syncwarp();
+        if (valid && (peers >> lane) == 1u) {
+          wm[d] = 0u;
+          wh[d] = before + (u32)__popc(peers);
+        }
+        rank = before + (u32)__popc(peers & lt);
+      }
+      __syncwarp();
+    }
+    rd[i] = valid ? (d << 16) | rank : kNoRank;
+  }
+}
+
 // Where the first pass reads payload word w of row r: *(u32*)(ptr + r*stride + off);
 // a null ptr means the row id itself.
 struct PayloadSrc {
@@ -647,7 +701,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     // atomics, digit or row-slot arrays in shared memory.
     u32* wh = whist + warp * RADIX;
     if constexpr (L::OR_RANK) {
-      warp_rank_or<IPT, RADIX>(rd, wh, wmask + warp * RADIX, lane);
+      warp_rank_mixed<IPT, RADIX, RB>(rd, wh, wmask + warp * RADIX, lane);
 #pragma unroll
       for (int i = 0; i < IPT; ++i)
         rd[i] = rd[i] != kNoRank ? 0x80000000u | ((rd[i] >> 16) << 13) | (rd[i] & 0xffffu) : 0u;
