@@ -1437,7 +1437,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     rq.key_mode = KEY_PACK;
     rq.digit_mode = DIG_BITS;
     rq.key64 = false;
-    rq.max_digit_bits = 9;  // 17 bucket bits at 2^28 rows: two passes of 9 + 8 bits
+    rq.max_digit_bits = 9;  // 18 bucket bits at 2^28 rows: two passes of 9 bits
     rq.nwords = 3;
     rq.pfirst[0] = PayloadSrc{(const unsigned char*)keys, 8u, 0u};
     rq.pfirst[1] = PayloadSrc{(const unsigned char*)keys, 8u, 4u};
