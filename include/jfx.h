@@ -221,7 +221,7 @@ int jfx_hash_partition(const jfx_column* keys, int ncols, int64_t n, int num_par
  * the stable int32 permutation).  A 1% strided sample, sorted by the plain
  * radix sort, trains a two-level piecewise-linear model (root line plus 4096
  * leaf lines, least squares) of each key's position.  The predicted
- * position's top bits name a bucket of about 1024 rows; two stable radix
+ * position's top bits name a bucket of about 2048 rows; two stable radix
  * passes over the bucket id move (key, row id) into bucket order, and each
  * bucket is then sorted by key inside one CTA (a bucket too large for shared
  * memory by one CTA in global memory, or above 2^20 rows by the plain radix

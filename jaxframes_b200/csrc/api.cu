@@ -273,7 +273,7 @@ static void carve_learned(Arena& ar, u64 n, Common& c, SortBuffers& b, LearnedBu
   l.last = ar.take<u32>(kLeaves);
   l.fit = ar.take<double>(2 * kLeaves);
   l.flags = ar.take<u32>(8);
-  l.nb = ((4 * n) >> kBucketShift) + 1;  // positions lie in [0, 4n)
+  l.nb = n ? ((4 * n - 1) >> kBucketShift) + 1 : 1;  // positions lie in [0, 4n)
   l.starts = ar.take<u32>(l.nb + 1);
   l.large = ar.take<u32>(2 * kBucketLargeMax);
   l.cap_chunks = n / kLargeChunk + kBucketLargeMax + 1;
@@ -1437,7 +1437,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
     rq.key_mode = KEY_PACK;
     rq.digit_mode = DIG_BITS;
     rq.key64 = false;
-    rq.max_digit_bits = 9;  // 18 bucket bits at 2^28 rows: two passes of 9 bits
+    rq.max_digit_bits = 9;  // 17 bucket bits at 2^28 rows: two passes of 9 + 8 bits
     rq.nwords = 3;
     rq.pfirst[0] = PayloadSrc{(const unsigned char*)keys, 8u, 0u};
     rq.pfirst[1] = PayloadSrc{(const unsigned char*)keys, 8u, 4u};

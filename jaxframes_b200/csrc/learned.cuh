@@ -9,7 +9,7 @@
 //    (radix.cuh: model_pos).  Slopes are forced >= 0 and leaf ranges are
 //    disjoint and increasing, so the predicted position is monotone in x;
 //    k_leaf_finalize verifies it.
-// 3. The predicted position's top bits name a bucket of about 1024 rows.
+// 3. The predicted position's top bits name a bucket of about 2048 rows.
 //    Two stable radix passes over the bucket id (not over the key's 64 bits)
 //    move (key, row id) pairs into bucket order, row order inside a bucket.
 // 4. The model is monotone, so every key of a bucket is <= every key of the
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256) k_model_positions(const u64* keys, u64 n,
 }
 
 // ------------------------------------------------------------- buckets ---
-constexpr int kBucketShift = 12;  // positions in [0, 4n): 4096 positions, about 1024 rows, per bucket
+constexpr int kBucketShift = 13;  // positions in [0, 4n): 8192 positions, about 2048 rows, per bucket
 constexpr int kBucketThreads = 256, kBucketIPT = 16;
 constexpr u32 kBucketCap = kBucketThreads * kBucketIPT;  // rows one CTA sorts in shared memory
 constexpr u32 kBucketSmallCap = kBucketThreads * 8;       // buckets the 8-item instantiation takes

@@ -531,7 +531,19 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
                             (a.key_mode == KEY_PACK || a.key_mode == KEY_MODEL) && !a.gather_idx;
   // this thread's first slot in the tile; item i sits at toff + 32 i
   const u32 toff = warp * 32 * IPT + lane;
-  if (!FIRST && full) {
+  // A later two-phase pass of 32-bit keys with one payload word moves each
+  // full tile's (key, payload) pairs through shared memory as one 64-bit word
+  // (PACK): the payload is loaded into registers instead of being staged, so
+  // the tile costs one random shared-memory store per row instead of two
+  // plus the staging writes and reads.
+  constexpr bool PACK = TP && FM == 0 && sizeof(K) == 4 && NW == 1;
+  static_assert(!PACK || L::A_BYTES + L::PAY_BYTES >= (size_t)TILE * 8, "packed tile fits");
+  u32 pay_reg[PACK ? IPT : 1];
+  if (PACK && full) {
+    const u32* src = a.vin[0] + base + toff;
+#pragma unroll
+    for (int i = 0; i < (PACK ? IPT : 0); ++i) pay_reg[i] = __ldg(src + i * 32);
+  } else if (!FIRST && full) {
     // later pass, full tile: per-thread base pointers, immediate offsets
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
@@ -750,6 +762,45 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
       if (rd[i] & 0x80000000u) {
         const u32 d = (rd[i] >> 13) & 0x7ffu;
         rd[i] = 0x80000000u | (sexcl[d] + wh[d] + (rd[i] & 0x1fffu));  // tile-local sorted slot
+      }
+    }
+    if constexpr (PACK) {
+      if (full) {
+        u64* skp = (u64*)smem;  // [TILE] key | payload << 32, over the histogram and staging bytes
+        __syncthreads();        // every whist read is done
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+          if (rd[i] & 0x80000000u) skp[rd[i] & 0x1fffu] = (u64)(u32)key[i] | ((u64)pay_reg[i] << 32);
+        __syncthreads();
+        K* kout = (K*)a.keys_out;
+        const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+        const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
+#pragma unroll
+        for (int i0 = 0; i0 < IPT; i0 += 8) {
+          u64 kp[8];
+          u32 gg[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const u32 j = (i0 + i) * THREADS + tid;
+            kp[i] = skp[j];
+            gg[i] = sbase[((u32)kp[i] >> a.shift) & mask] + j;
+          }
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            if (gg[i] - row0 >= span) {
+              atomicOr(a.err, DERR_BOUNDS);
+              continue;
+            }
+            const K k = (K)(u32)kp[i];
+            const u64 g = a.reverse ? a.n - 1 - (u64)gg[i] : (u64)gg[i];
+            if (rsz) store_raw(a.raw_out, a.raw_dtype, g, untransform_int(a.raw_dtype, a.raw_flags, (u64)k + a.raw_tmin));
+            else kout[g] = k;
+            a.vout[0][g] = (u32)(kp[i] >> 32);
+          }
+        }
+        if (a.status_next)
+          for (int d = tid; d < RADIX; d += THREADS) a.status_next[(u64)tile * RADIX + d] = 0u;
+        return;
       }
     }
     cp_async_wait_all();
