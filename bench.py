@@ -111,11 +111,11 @@ def c4_keys(nblocks=65_536, block=4096, seed=45):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one
 # k_onesweep launch of this workload, averaged over the six radix passes of
-# one join call: 541.8 MB over 6 launches in an ncu capture of those launches
+# one join call: 544.7 MB over 6 launches in an ncu capture of those launches
 # (`--metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:k_onesweep
 # -s 30 -c 6` around `bench.py --profile --steps 1 --warmup 5`); the writes
 # that are still in L2 when a launch ends are not counted.
-ONESWEEP_DRAM_BYTES_PER_LAUNCH = 90.3e6
+ONESWEEP_DRAM_BYTES_PER_LAUNCH = 90.8e6
 
 
 def join_model_bytes(nl, nr, m):

@@ -249,7 +249,9 @@ int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out,
  *   of query q at [group_offsets_out[q], group_offsets_out[q+1]), keys
  *   ascending.
  * Keys must lie in [0, 2^key_bits); jfx_batch_status reports a violation.
- * ceil(log2(nq)) + key_bits must not exceed 32. */
+ * One persistent kernel launch does all of it: a device work queue of the
+ * queries, largest first, each query's partition, sort and groupby run by
+ * one CTA. */
 int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const int64_t* query_offsets,
                                 int nq, int64_t n, int num_partitions, int key_bits,
                                 int32_t* part_keys_out, float* part_values_out,

@@ -134,7 +134,9 @@ static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream
   JFX_CUDA(cudaGetLastError());
   JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
   JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
-  k_group_reduce<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
+  static SmemAttr attr;
+  JFX_TRY(ensure_smem(attr, k_group_reduce<K>, kGroupStageBytes));
+  k_group_reduce<K><<<blocks, 256, kGroupStageBytes, s>>>(ga, g.nwarps), note_launch();
   JFX_CUDA(cudaGetLastError());
   k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
   JFX_CUDA(cudaGetLastError());
@@ -343,48 +345,29 @@ static int sort_rows_u64(u64* keys, u32* ids, u64 m, u64 kmin, int bits, u64* tk
 
 // ------------------------------------------------------------------ batch ---
 struct BatchBuffers {
-  u64* row_base;
-  u32* tile_cnt;
-  u32* tile_base;
-  u32* total_tiles;
-  u32* scan_part;
-  u32* tile_seg;
-  u32* hist;
-  u32* base;
-  u32* counters;
-  u32* status[2];
-  u32* keys[2];
-  u32* vals[2];
-  u32* sk;
-  u32* sv;
-  u32* group_q;
-  GroupBuffers g;
-  u64 max_tiles;
+  u32* sk[2];
+  u32* sv[2];
+  u32* tkeys;
+  double* tsums;
+  u32* tcnts;
+  u32* qgroups;
+  u32* order;
+  u32* ctl;
 };
 
 static void carve_batch(Arena& ar, u64 n, u64 nq, Common& c, BatchBuffers& b) {
-  take_common(ar, c);
+  take_common(ar, c);  // the error word opens the workspace (jfx_batch_status)
   const u64 nn = n ? n : 1;
-  b.max_tiles = n / kBatchTile + nq + 1;
-  b.row_base = ar.take<u64>(nq + 2);
-  b.tile_cnt = ar.take<u32>(nq + 2);
-  b.tile_base = ar.take<u32>(nq + 2);
-  b.total_tiles = ar.take<u32>(4);
-  b.scan_part = ar.take<u32>(scan_partials_count(nq + 1));
-  b.tile_seg = ar.take<u32>(b.max_tiles);
-  b.hist = ar.take<u32>((nq + 1) * 4 * (1u << kBatchRB));
-  b.base = ar.take<u32>((nq + 1) * 4 * (1u << kBatchRB));
-  b.counters = ar.take<u32>(64);
-  b.status[0] = ar.take<u32>(b.max_tiles * (1u << kBatchRB));
-  b.status[1] = ar.take<u32>(b.max_tiles * (1u << kBatchRB));
-  b.keys[0] = ar.take<u32>(nn);
-  b.keys[1] = ar.take<u32>(nn);
-  b.vals[0] = ar.take<u32>(nn);
-  b.vals[1] = ar.take<u32>(nn);
-  b.sk = ar.take<u32>(nn);
-  b.sv = ar.take<u32>(nn);
-  b.group_q = ar.take<u32>(nn);
-  take_group_buffers(ar, n, 1, b.g);
+  for (int i = 0; i < 2; ++i) {
+    b.sk[i] = ar.take<u32>(nn);
+    b.sv[i] = ar.take<u32>(nn);
+  }
+  b.tkeys = ar.take<u32>(nn);
+  b.tsums = ar.take<double>(nn);
+  b.tcnts = ar.take<u32>(nn);
+  b.qgroups = ar.take<u32>(nq + 1);
+  b.order = ar.take<u32>(nq + 1);
+  b.ctl = ar.take<u32>(64);
 }
 
 // -------------------------------------------------------------- partition ---
@@ -1565,9 +1548,6 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   if (nq < 1) return fail(JFX_ERR_ARG, "need at least one query");
   if (num_partitions < 1 || num_partitions > 256) return fail(JFX_ERR_ARG, "num_partitions must be in [1, 256]");
   if (key_bits < 1 || key_bits > 30) return fail(JFX_ERR_ARG, "key_bits must be in [1, 30]");
-  const int qbits = std::max(1, bit_length((u64)(nq - 1)));
-  if (qbits + key_bits > 32)
-    return fail(JFX_ERR_CAPACITY, "query id (%d bits) and key (%d bits) exceed 32 bits", qbits, key_bits);
   if (!keys || !values || !query_offsets || !part_keys_out || !part_values_out || !part_offsets_out ||
       !group_keys_out || !group_sums_out || !group_counts_out || !group_offsets_out)
     return fail(JFX_ERR_ARG, "null pointer");
@@ -1577,150 +1557,43 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   BatchBuffers bb;
   carve_batch(ar, (u64)n, (u64)nq, c, bb);
   JFX_TRY(check_workspace(ar, workspace, workspace_bytes));
-  constexpr int RB = kBatchRB, RADIX = 1 << RB;
+  // one persistent launch: as many CTAs as are resident at once
+  static SmemAttr attr;
+  const size_t smem = sizeof(QueueShared);
+  JFX_TRY(ensure_smem(attr, k_batch_queue, smem));
+  int per_sm = 0;
+  JFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_queue, kQueueThreads, smem));
+  const int grid = std::max(1, std::min(per_sm * device_sm_count(), nq));
   JFX_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s));
-  // segment tables
-  const int gq = grid_for((u64)nq + 1, 256);
-  k_seg_setup<<<gq, 256, 0, s>>>(query_offsets, (u32)nq, bb.row_base, bb.tile_cnt, c.err), note_launch();
-  JFX_TRY(device_exclusive_scan<u32>(bb.tile_cnt, (u64)nq, bb.tile_base, bb.total_tiles, bb.scan_part, s));
-  JFX_CUDA(cudaMemcpyAsync(bb.tile_base + nq, bb.total_tiles, sizeof(u32), cudaMemcpyDeviceToDevice, s));
-  k_seg_tile_map<<<gq, 256, 0, s>>>(bb.tile_base, bb.tile_cnt, (u32)nq, bb.tile_seg), note_launch();
-  // histograms of the partition digit and the key digits, per query
-  const int npk = ceil_div(key_bits, RB);
-  const int npass = 1 + npk;
-  int shift[8] = {0}, width[8] = {0};
-  width[0] = 8;
-  {
-    const int bw = key_bits / npk, rem = key_bits % npk;
-    int at = 0;
-    for (int p = 1; p <= npk; ++p) {
-      width[p] = bw + (p - 1 < rem ? 1 : 0);
-      shift[p] = at;
-      at += width[p];
-    }
+  JFX_CUDA(cudaMemsetAsync(bb.ctl, 0, 64 * sizeof(u32), s));
+  QueueArgs qa;
+  qa.keys = keys;
+  qa.values = values;
+  qa.qoff = query_offsets;
+  qa.n = (u64)n;
+  qa.nq = (u32)nq;
+  qa.P = (u32)num_partitions;
+  qa.key_bits = key_bits;
+  qa.part_keys = part_keys_out;
+  qa.part_values = part_values_out;
+  qa.part_offsets = part_offsets_out;
+  qa.group_keys = group_keys_out;
+  qa.group_sums = group_sums_out;
+  qa.group_counts = group_counts_out;
+  qa.group_offsets = group_offsets_out;
+  for (int i = 0; i < 2; ++i) {
+    qa.sk[i] = bb.sk[i];
+    qa.sv[i] = bb.sv[i];
   }
-  JFX_CUDA(cudaMemsetAsync(bb.hist, 0, (size_t)nq * npass * RADIX * sizeof(u32), s));
-  JFX_CUDA(cudaMemsetAsync(bb.counters, 0, 64 * sizeof(u32), s));
-  {
-    SegHistArgs h;
-    memset(&h, 0, sizeof h);
-    h.keys = keys;
-    h.row_base = bb.row_base;
-    h.tile_base = bb.tile_base;
-    h.tile_seg = bb.tile_seg;
-    h.total_tiles = bb.total_tiles;
-    h.hist = bb.hist;
-    h.err = c.err;
-    h.npass = npass;
-    h.modulus = (u32)num_partitions;
-    h.key_bits = key_bits;
-    for (int p = 0; p < 8; ++p) {
-      h.shift[p] = shift[p];
-      h.width[p] = width[p];
-    }
-    static SmemAttr attr;
-    JFX_TRY(ensure_smem(attr, k_hist_seg<RB>, 4 * RADIX * 4));
-    k_hist_seg<RB><<<device_sm_count() * 4, 256, npass * RADIX * sizeof(u32), s>>>(h), note_launch();
-  }
-  k_hist_scan<RB><<<(unsigned)(nq * npass), 1024, 0, s>>>(bb.hist, bb.base), note_launch();
-  JFX_CUDA(cudaMemsetAsync(bb.status[0], 0, bb.max_tiles * RADIX * sizeof(u32), s));
-  JFX_CUDA(cudaGetLastError());
-  // pass 0: stable partition by fmix32(key) % P, moving (key, value)
-  PassArgs a;
-  memset(&a, 0, sizeof a);
-  a.n = (u64)n;
-  a.err = c.err;
-  a.segmented = 1;
-  a.seg.row_base = bb.row_base;
-  a.seg.tile_base = bb.tile_base;
-  a.seg.tile_seg = bb.tile_seg;
-  a.seg.nseg = (u32)nq;
-  a.seg.total_tiles = bb.total_tiles;
-  a.seg.npass_stride = npass;
-  a.bin_base = bb.base;
-  {
-    jfx_column col{keys, JFX_I32, 0u};
-    JFX_TRY(build_pack(&col, 1, 0u, false, a.pack));
-    a.pack.c[0].bits = 32;
-  }
-  a.key_mode = KEY_PACK;
-  a.digit_mode = DIG_HASHMOD;
-  a.modulus = (u32)num_partitions;
-  a.width = RB;
-  a.pfirst[0].ptr = (const unsigned char*)values;
-  a.pfirst[0].stride = 4;
-  a.raw_out = part_keys_out;
-  a.raw_dtype = JFX_I32;
-  a.keys_out = bb.keys[0];
-  a.vout[0] = (u32*)part_values_out;
-  a.status = bb.status[0];
-  a.status_next = bb.status[1];
-  a.tile_counter = bb.counters;
-  a.seg.pass_index = 0;
-  JFX_TRY((launch_pass<u32, RB, 1>(a, (u64)n, s, bb.max_tiles)));  // one plain int32 key column
-  {
-    const u64 tot = (u64)nq * (num_partitions + 1);
-    k_part_offsets<<<grid_for(tot, 256), 256, 0, s>>>(bb.row_base, bb.base, (u32)nq, npass, RADIX,
-                                                     (u32)num_partitions, part_offsets_out), note_launch();
-  }
-  // key passes over the partitioned rows, values carried
-  const u32* kin = (const u32*)part_keys_out;
-  const u32* vin = (const u32*)part_values_out;
-  for (int p = 1; p <= npk; ++p) {
-    const bool last = p == npk;
-    PassArgs b = a;
-    b.pfirst[0].ptr = nullptr;
-    b.raw_out = nullptr;
-    b.digit_mode = DIG_BITS;
-    b.shift = shift[p];
-    b.width = width[p];
-    b.keys_in = kin;
-    b.vin[0] = vin;
-    b.keys_out = last ? bb.sk : bb.keys[p & 1];
-    b.vout[0] = last ? bb.sv : bb.vals[p & 1];
-    b.status = bb.status[p & 1];
-    b.status_next = last ? nullptr : bb.status[(p + 1) & 1];
-    b.tile_counter = bb.counters + p;
-    b.seg.pass_index = p;
-    b.seg.key_shift_q = last ? key_bits : 0;
-    JFX_TRY((launch_pass<u32, RB, 0>(b, (u64)n, s, bb.max_tiles)));
-    kin = (const u32*)b.keys_out;
-    vin = b.vout[0];
-  }
-  // groupby sum and count over the whole batch on (query, key) composite keys
-  GroupArgs ga;
-  memset(&ga, 0, sizeof ga);
-  ga.skeys = bb.sk;
-  ga.perm = nullptr;
-  ga.values_sorted = 1;
-  ga.n = (u64)n;
-  ga.warp_count = bb.g.warp_count;
-  ga.warp_base = bb.g.warp_base;
-  ga.pack.ncols = 2;
-  ga.pack.c[0].dtype = JFX_U32;
-  ga.pack.c[0].shift = key_bits;
-  ga.pack.c[0].bits = qbits;
-  ga.pack.c[1].dtype = JFX_I32;
-  ga.pack.c[1].shift = 0;
-  ga.pack.c[1].bits = key_bits;
-  ga.pack.c[1].tmin = 0x80000000ull;
-  ga.uniq_out[0] = bb.group_q;
-  ga.uniq_out[1] = group_keys_out;
-  ga.nvals = 1;
-  ValDesc& v = ga.v[0];
-  v.ptr = bb.sv;
-  v.dtype = JFX_F32;
-  v.kind = VK_F;
-  v.aggs = JFX_AGG_SUM | JFX_AGG_COUNT;
-  v.count_dtype = JFX_F32;
-  v.out_sum = group_sums_out;
-  v.out_count = group_counts_out;
-  if (n) {
-    JFX_TRY(launch_group_reduce<u32>(ga, bb.g, (u64)n, s));
-  } else {
-    JFX_CUDA(cudaMemsetAsync(bb.g.total, 0, sizeof(u32), s));
-  }
-  k_group_offsets<<<gq, 256, 0, s>>>(bb.group_q, bb.g.total, (u32)nq, group_offsets_out), note_launch();
+  qa.tkeys = bb.tkeys;
+  qa.tsums = bb.tsums;
+  qa.tcnts = bb.tcnts;
+  qa.qgroups = bb.qgroups;
+  qa.order = bb.order;
+  qa.ctl = bb.ctl;
+  qa.err = c.err;
+  qa.spin_ns = (u64)g_tuning.spin_limit_us * 1000ull;
+  k_batch_queue<<<grid, kQueueThreads, smem, s>>>(qa), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }

@@ -182,20 +182,6 @@ enum : int {
   DIG_BITS = 0,   // digit = (key >> shift) & mask
   DIG_MOD = 1,    // digit = key % modulus (hash partition)
   DIG_MODEL = 2,  // digit = (model position of key >> shift) & mask (learned sort)
-  DIG_HASHMOD = 3,  // digit = fmix32(key) % modulus (partition that moves the raw key)
-};
-
-// Segmented passes (batched queries): tiles never straddle a segment, the
-// look-back chains only within a segment and digit offsets are per segment.
-struct SegTables {
-  const u64* row_base;   // [nseg + 1] first row of each segment
-  const u32* tile_base;  // [nseg + 1] first tile id of each segment
-  const u32* tile_seg;   // [tiles] segment of each tile
-  u32 nseg;
-  const u32* total_tiles;  // device: number of real tiles (the grid is an upper bound)
-  int npass_stride;      // passes per segment in the histogram layout
-  int pass_index;        // this pass's index in that layout
-  int key_shift_q;       // > 0: the last pass writes key | (segment << key_shift_q)
 };
 
 // ---- learned-CDF model (fitted in learned.cuh), evaluated inside the passes
@@ -262,8 +248,6 @@ struct PassArgs {
   u64 raw_tmin;
   const ModelRef* model; // DIG_MODEL / KEY_MODEL: device-resident model
   unsigned long long* vout64;  // last pass: payload words 0 and 1 written as one u64 here
-  int segmented;
-  SegTables seg;
   PackDesc pack;
   // two-phase pass: [RADIX][tiles] global position of each tile's first key
   // of each digit, computed beforehand (k_tile_count + k_tile_scan); the
@@ -330,7 +314,6 @@ __device__ __forceinline__ u32 fmix32_d(u32 h) {
 template <typename K>
 __device__ __forceinline__ u32 digit_of(K key, int mode, int shift, u32 mask, u32 modulus, const ModelRef& m) {
   if (mode == DIG_MOD) return (u32)key % modulus;
-  if (mode == DIG_HASHMOD) return fmix32_d((u32)key ^ 0x80000000u) % modulus;
   if (mode == DIG_MODEL) return (model_pos(m, (u64)key) >> shift) & mask;
   return (u32)(key >> shift) & mask;
 }
@@ -463,7 +446,7 @@ __device__ __forceinline__ K pack2(const PackDesc& pd, u64 r0, u64 r1) {
 // instantiation: fewer registers, more CTAs per SM); 2 = any other first pass
 // (packed or hashed columns, gathered rows, the learned position).
 // TP: a two-phase pass over plain bit digits (PassArgs::tile_base set,
-// DIG_BITS, not segmented); otherwise the tile bases come from the look-back.
+// DIG_BITS); otherwise the tile bases come from the look-back.
 template <typename K, int RB, int FM, int NW, bool TP>
 __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs a) {
   constexpr bool FIRST = FM != 0;
@@ -503,21 +486,10 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   }
   __syncthreads();
   const u32 tile = sflag[0];
-  // segment of the tile: rows [seg_row0, seg_row1), tiles from seg_tile0
-  u32 q = 0, seg_tile0 = 0;
-  u64 seg_row0 = 0, seg_row1 = a.n;
   const u32* bin_base = a.bin_base;
-  if (a.segmented) {
-    if (tile >= *a.seg.total_tiles) return;  // surplus CTA (the grid is an upper bound)
-    q = a.seg.tile_seg[tile];
-    seg_row0 = a.seg.row_base[q];
-    seg_row1 = a.seg.row_base[q + 1];
-    seg_tile0 = a.seg.tile_base[q];
-    bin_base = a.bin_base + ((u64)q * a.seg.npass_stride + a.seg.pass_index) * RADIX;
-  }
-  const u64 base = seg_row0 + (u64)(tile - seg_tile0) * TILE;
-  const u32 tile_n = (u32)min((u64)TILE, seg_row1 - base);
-  const bool first_tile = tile == seg_tile0;
+  const u64 base = (u64)tile * TILE;
+  const u32 tile_n = (u32)min((u64)TILE, a.n - base);
+  const bool first_tile = tile == 0;
   const u32 mask = a.width >= 32 ? 0xffffffffu : ((1u << a.width) - 1u);
   const bool full = tile_n == (u32)TILE;
   ModelRef model;
@@ -755,7 +727,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
 #pragma unroll
     for (int k = 0; k < DPT; ++k) {
       const int d = tid + k * THREADS;
-      if (d < RADIX) sbase[d] = (u32)seg_row0 + tb_pre[k] - sexcl[d];
+      if (d < RADIX) sbase[d] = tb_pre[k] - sexcl[d];
     }
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
@@ -773,7 +745,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
           if (rd[i] & 0x80000000u) skp[rd[i] & 0x1fffu] = (u64)(u32)key[i] | ((u64)pay_reg[i] << 32);
         __syncthreads();
         K* kout = (K*)a.keys_out;
-        const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+        const u32 row0 = 0u, span = (u32)a.n;
         const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
 #pragma unroll
         for (int i0 = 0; i0 < IPT; i0 += 8) {
@@ -821,7 +793,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     __syncthreads();
 
     K* kout = (K*)a.keys_out;
-    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+    const u32 row0 = 0u, span = (u32)a.n;
     const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
     const bool plain = !a.raw_out && !a.reverse;
     if (full) {
@@ -925,19 +897,19 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   constexpr int WIN = (RADIX / THREADS) >= 8 ? 4 : (RADIX / THREADS) >= 4 ? 8 : 16;
   for (int d = tid; d < RADIX; d += THREADS) {
     if (a.tile_base) {  // two-phase pass: the tile's digit bases are known
-      sbase[d] = (u32)seg_row0 + a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
+      sbase[d] = a.tile_base[(u64)d * a.ntiles + tile] - sexcl[d];
       continue;
     }
     const u32 c = sbase[d];
     u32 excl = 0;
     bool bad = false;
     if (!first_tile) {
-      excl = lookback_window<WIN>(a.status, tile, seg_tile0, (u32)d, (u32)RADIX, a.err, a.spin_ns, bad);
+      excl = lookback_window<WIN>(a.status, tile, 0u, (u32)d, (u32)RADIX, a.err, a.spin_ns, bad);
       if (tile != a.withhold_tile) st_relaxed(st + d, bad ? ST_ERR : (ST_INC | (excl + c)));
     }
     if (bad) sflag[1] = 1u;
     // global position of the tile's sorted index j is sbase[d] + j (mod 2^32)
-    sbase[d] = (u32)seg_row0 + bin_base[d] + excl - sexcl[d];
+    sbase[d] = bin_base[d] + excl - sexcl[d];
   }
 
   // Stable rank within the tile: lanes holding the same digit are ranked by
@@ -991,9 +963,9 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   if (sflag[1]) return;
 
   K* kout = (K*)a.keys_out;
-  const bool plain_out = !a.raw_out && !a.reverse && !(a.segmented && a.seg.key_shift_q);
+  const bool plain_out = !a.raw_out && !a.reverse;
   if (full && plain_out) {
-    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+    const u32 row0 = 0u, span = (u32)a.n;
     // full tile: IPT independent slots per thread, loads before stores
 #pragma unroll
     for (int i0 = 0; i0 < IPT; i0 += 8) {
@@ -1031,7 +1003,7 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
   if (full) {
     // full tile, other output forms (original-dtype keys, descending
     // positions, query-tagged keys): the same unrolled slots
-    const u32 row0 = (u32)seg_row0, span = (u32)(seg_row1 - seg_row0);
+    const u32 row0 = 0u, span = (u32)a.n;
     const int rsz = a.raw_out ? dtype_size(a.raw_dtype) : 0;
 #pragma unroll
     for (int i0 = 0; i0 < IPT; i0 += 8) {
@@ -1056,8 +1028,6 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
           if (rsz == 4) ((u32*)a.raw_out)[g] = (u32)v;
           else if (rsz == 8) ((u64*)a.raw_out)[g] = v;
           else store_raw(a.raw_out, a.raw_dtype, g, v);
-        } else if (a.segmented && a.seg.key_shift_q) {
-          kout[g] = (kk[i] & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
         } else {
           kout[g] = kk[i];
         }
@@ -1080,14 +1050,12 @@ __global__ void __launch_bounds__(RadixCfg<RB, NW>::THREADS) k_onesweep(PassArgs
     const u32 d = sdig[j];
     const u32 u = sidx[j];
     u64 g = (u64)(u32)(sbase[d] + j);
-    if (g < seg_row0 || g >= seg_row1) {  // only reachable if histogram and pass disagree
+    if (g >= a.n) {  // only reachable if histogram and pass disagree
       atomicOr(a.err, DERR_BOUNDS);
       continue;
     }
     if (a.reverse) g = a.n - 1 - g;
     if (a.raw_out) store_raw(a.raw_out, a.raw_dtype, g, untransform_int(a.raw_dtype, a.raw_flags, (u64)k + a.raw_tmin));
-    else if (a.segmented && a.seg.key_shift_q)
-      kout[g] = (k & (((K)1 << a.seg.key_shift_q) - 1)) | ((K)q << a.seg.key_shift_q);
     else kout[g] = k;
     if (NW >= 2 && a.vout64) {
       a.vout64[g] = (unsigned long long)spay[u] | ((unsigned long long)spay[TILE + u] << 32);
@@ -1906,7 +1874,7 @@ template <typename K, int RB, int FM, int NW = 1, bool TP = false>
 inline int launch_pass(const PassArgs& a, u64 n, cudaStream_t s, u64 grid_tiles = 0) {
   constexpr bool FIRST = FM != 0;
   using L = PassLayout<K, RB, NW>;
-  if (TP && (!a.tile_base || a.digit_mode != DIG_BITS || a.segmented))
+  if (TP && (!a.tile_base || a.digit_mode != DIG_BITS))
     return fail(JFX_ERR_ARG, "two-phase pass without tile bases or with non-bit digits");
   static SmemAttr attr;  // per instantiation
   JFX_TRY(ensure_smem(attr, k_onesweep<K, RB, FM, NW, TP>, L::SMEM));
@@ -2143,7 +2111,7 @@ inline int run_radix(RadixRequest& rq, u64 n, SortBuffers& b, u32* err, cudaStre
       a.ntiles = tiles;
       a.status = nullptr;
     }
-    const bool tp = a.tile_base != nullptr;  // two-phase (plain bit digits, not segmented)
+    const bool tp = a.tile_base != nullptr;  // two-phase (plain bit digits)
     if (p == 0 && int1) {
       JFX_TRY(tp ? (launch_pass<K, RB, 1, NW, true>(a, n, s)) : (launch_pass<K, RB, 1, NW, false>(a, n, s)));
     } else if (p == 0) {
