@@ -134,9 +134,7 @@ static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream
   JFX_CUDA(cudaGetLastError());
   JFX_TRY(device_exclusive_scan<u32>(g.warp_count, g.nwarps, g.warp_base, g.total, g.partial, s));
   JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
-  static SmemAttr attr;
-  JFX_TRY(ensure_smem(attr, k_group_reduce<K>, kGroupStageBytes));
-  k_group_reduce<K><<<blocks, 256, kGroupStageBytes, s>>>(ga, g.nwarps), note_launch();
+  k_group_reduce<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
   JFX_CUDA(cudaGetLastError());
   k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
   JFX_CUDA(cudaGetLastError());

@@ -341,38 +341,6 @@ __device__ __forceinline__ u64 carried_word(const ValDesc& v, u32 lo, u32 hi) {
   return (u64)lo;
 }
 
-// A warp's groups that start and end inside its rows, staged in shared
-// memory at their index among the warp's group starts (at most 32 *
-// kGroupIPT), so that the group writes run afterwards with every lane
-// active on consecutive group ids instead of one lane at a time inside the
-// row walk.  The key columns of the group starts use the same space first
-// (sum: packed key, cnt: row).
-struct GroupStage {
-  u64 sum[32 * kGroupIPT];
-  u64 mn[32 * kGroupIPT];
-  u64 mx[32 * kGroupIPT];
-  u32 cnt[32 * kGroupIPT];
-};
-constexpr size_t kGroupStageBytes = 8 * sizeof(GroupStage);  // 256-thread CTA: 8 warps
-
-template <int KIND>
-__device__ __forceinline__ void stage_put(GroupStage* st, u32 li, const Agg<KIND>& s) {
-  st->sum[li] = s.sum;
-  st->mn[li] = s.mn;
-  st->mx[li] = s.mx;
-  st->cnt[li] = s.cnt;
-}
-
-template <int KIND>
-__device__ __forceinline__ Agg<KIND> stage_get(const GroupStage* st, u32 li) {
-  Agg<KIND> s;
-  s.sum = st->sum[li];
-  s.mn = st->mn[li];
-  s.mx = st->mx[li];
-  s.cnt = st->cnt[li];
-  return s;
-}
-
 // One value column over the warp's rows, lane-sequential: lane l owns the
 // kGroupIPT consecutive rows r0.. (bit j of fl: row r0+j starts a group).
 // Pass 1 folds each lane's rows after its last group start; a segmented
@@ -383,8 +351,7 @@ __device__ __forceinline__ Agg<KIND> stage_get(const GroupStage* st, u32 li) {
 template <int KIND>
 __device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u64 w, u64 r0, int nv, u32 fl,
                                                    u32 gfirst, bool last_lane, bool end_closes, bool next_flag,
-                                                   const u32 (&pr)[kGroupIPT], GroupStage* st, u32 wgid,
-                                                   u32 nfinal) {
+                                                   const u32 (&pr)[kGroupIPT]) {
   const ValDesc& v = a.v[c];
   const int lane = threadIdx.x & 31;
   const bool need_vals = (v.aggs & ~JFX_AGG_COUNT) != 0;
@@ -446,18 +413,12 @@ __device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u6
     cur_started = false;
   }
   u32 cur_gid = gfirst - 1u;
-  // pass 2: write every group that ends inside the lane.  The loop is not
-  // unrolled (the group writes are long); the row's value is always word[0]
-  // and the words shift down one place per row, so the array stays in
-  // registers instead of being indexed at run time.
+  // pass 2: write every group that ends inside the lane
 #pragma unroll 1
   for (int j = 0; j < nv; ++j) {
-    const u64 wj = word[0];
-#pragma unroll
-    for (int t = 0; t + 1 < kGroupIPT; ++t) word[t] = word[t + 1];
     if ((fl >> j) & 1u) {
       if (cur_rows) {
-        if (cur_started) stage_put<KIND>(st, cur_gid - wgid, cur);
+        if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
         else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);  // the warp's first group, begun earlier
       }
       cur = agg_identity<KIND>();
@@ -466,28 +427,23 @@ __device__ __forceinline__ void reduce_lane_column(const GroupArgs& a, int c, u6
     }
     Agg<KIND> r;
     r.cnt = 1;
-    r.sum = r.mn = r.mx = need_vals ? wj : 0ull;
+    r.sum = r.mn = r.mx = need_vals ? word[j] : 0ull;
     cur = agg_combine<KIND>(cur, r);
     cur_rows = true;
   }
+  if (nv == 0) return;
   // the group open at the lane end ends here if the next lane starts a group,
   // or at the warp end when the row after the warp starts one
-  if (nv > 0) {
-    if (last_lane ? end_closes : next_flag) {
-      if (cur_started) stage_put<KIND>(st, cur_gid - wgid, cur);
-      else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);
-    } else if (last_lane) {
-      slot_store<KIND>(a, c, 2 * w + 1, cur_gid, cur_started ? 1u : 0u, cur);  // open past the warp end
-    }
+  if (last_lane ? end_closes : next_flag) {
+    if (cur_started) agg_finalize<KIND>(v, cur_gid, cur);
+    else slot_store<KIND>(a, c, 2 * w, cur_gid, 0u, cur);
+  } else if (last_lane) {
+    slot_store<KIND>(a, c, 2 * w + 1, cur_gid, cur_started ? 1u : 0u, cur);  // open past the warp end
   }
-  // every group that starts and ends in the warp, lane-parallel
-  __syncwarp();
-  for (u32 li = (u32)lane; li < nfinal; li += 32) agg_finalize<KIND>(v, (u64)wgid + li, stage_get<KIND>(st, li));
-  __syncwarp();
 }
 
 template <typename K>
-__global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps) {  // 2 CTAs per SM
+__global__ void __launch_bounds__(256, 4) k_group_reduce(GroupArgs a, u64 nwarps) {  // 4 CTAs per SM
   const u64 w = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nwarps) return;  // whole warps exit together
@@ -530,58 +486,33 @@ __global__ void __launch_bounds__(256, 2) k_group_reduce(GroupArgs a, u64 nwarps
     const u32 y = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= o) inc += y;
   }
-  const u32 wgid = a.warp_base[w];  // id of the warp's first group start
-  const u32 gfirst = wgid + inc - cnt;
-  const u32 starts_w = __shfl_sync(0xffffffffu, inc, 31);
-  extern __shared__ __align__(16) unsigned char group_smem[];
-  GroupStage* st = reinterpret_cast<GroupStage*>(group_smem) + (threadIdx.x >> 5);
-  // unique key columns of every group starting in the warp: each start's
-  // packed key and row staged, then written lane-parallel
-  {
-    u64* skey = st->sum;
-    u32* srow = st->cnt;
-#pragma unroll
-    for (int j = 0; j < kGroupIPT; ++j) {
-      if ((fl >> j) & 1u) {
-        const u32 li = inc - cnt + __popc(fl & ((1u << j) - 1u));
-        skey[li] = (u64)kv[j];
-        srow[li] = (u32)(r0 + j);
+  const u32 gfirst = a.warp_base[w] + inc - cnt;
+  // unique key columns of every group starting in the lane
+  for (u32 m = fl; m; m &= m - 1) {
+    const int j = __ffs(m) - 1;
+    const u32 gid = gfirst + __popc(fl & ((1u << j) - 1u));
+    const u64 row = r0 + j;
+    for (int jc = 0; jc < a.pack.ncols; ++jc) {
+      const ColDesc& cd = a.pack.c[jc];
+      if (!a.uniq_out[jc]) continue;
+      if (dtype_is_float(cd.dtype)) {
+        // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
+        const u32 krow = a.perm ? a.perm[row] : (u32)row;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, load_raw(cd.ptr, cd.dtype, krow));
+      } else {
+        const u64 field = cd.bits ? (((u64)kv[j] >> cd.shift) & (cd.bits >= 64 ? ~0ull : ((1ull << cd.bits) - 1ull))) : 0ull;
+        store_raw(a.uniq_out[jc], cd.dtype, gid, untransform_int(cd.dtype, cd.flags, field + cd.tmin));
       }
     }
-    __syncwarp();
-    for (u32 li = (u32)lane; li < starts_w; li += 32) {
-      const u64 key = skey[li];
-      const u64 row = srow[li];
-      const u32 gid = wgid + li;
-      for (int jc = 0; jc < a.pack.ncols; ++jc) {
-        const ColDesc& cd = a.pack.c[jc];
-        if (!a.uniq_out[jc]) continue;
-        if (dtype_is_float(cd.dtype)) {
-          // original bits of the group's first row (-0.0 vs +0.0, NaN payloads)
-          const u32 krow = a.perm ? a.perm[row] : (u32)row;
-          store_raw(a.uniq_out[jc], cd.dtype, gid, load_raw(cd.ptr, cd.dtype, krow));
-        } else {
-          const u64 field = cd.bits ? ((key >> cd.shift) & (cd.bits >= 64 ? ~0ull : ((1ull << cd.bits) - 1ull))) : 0ull;
-          store_raw(a.uniq_out[jc], cd.dtype, gid, untransform_int(cd.dtype, cd.flags, field + cd.tmin));
-        }
-      }
-    }
-    __syncwarp();
   }
   const int last = (int)((wend - 1 - wbeg) / kGroupIPT);  // lane holding the warp's last row
   const bool end_closes = wend < a.n ? row_flag<K>(a, sk, wend) : true;
-  // groups staged per column: every start of the warp but the last when that
-  // group runs past the warp end
-  const u32 nfinal = (end_closes || starts_w == 0u) ? starts_w : starts_w - 1u;
   const bool next_flag = __shfl_down_sync(0xffffffffu, fl & 1u, 1) != 0u;
   for (int c = 0; c < a.nvals; ++c) {
     switch (a.v[c].kind) {
-      case VK_F: reduce_lane_column<VK_F>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr, st,
-                                              wgid, nfinal); break;
-      case VK_I: reduce_lane_column<VK_I>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr, st,
-                                              wgid, nfinal); break;
-      default: reduce_lane_column<VK_U>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr, st,
-                                              wgid, nfinal); break;
+      case VK_F: reduce_lane_column<VK_F>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      case VK_I: reduce_lane_column<VK_I>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
+      default: reduce_lane_column<VK_U>(a, c, w, r0, nv, fl, gfirst, lane == last, end_closes, next_flag, pr); break;
     }
   }
 }

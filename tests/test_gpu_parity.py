@@ -523,6 +523,36 @@ def test_batch_partition_groupby(P, P_):
     _check_batch(b, off, keys, vals, P_)
 
 
+@pytest.mark.parametrize("key_bits", [20, 28, 30])
+def test_batch_key_spreads(P, key_bits):
+    """Queries whose keys take each path of the per-query pipeline: one
+    bucket of 4096 keys (no bucket pass), 12/13-bit boundaries, one and two
+    bucket passes (keys over 20 bits), skewed buckets (many small buckets in
+    a chunk after a few large ones), and keys too sparse for buckets (sorted
+    by the whole key)."""
+    from jaxframes_b200.batch import batch_partition_groupby
+    rng = np.random.default_rng(key_bits)
+    top = 1 << key_bits
+    parts = [
+        rng.integers(0, 4096, 9000),                         # kbits 12: one bucket
+        np.full(5000, 4096),                                  # kbits 13, one key
+        rng.integers(0, 1 << 13, 30000),                      # one bucket pass, two buckets
+        rng.integers(0, min(top, 1 << 21), 600000),           # dense, 2 bucket passes when key_bits > 20
+        np.concatenate([rng.integers(0, 8192, 300000),        # skewed: two heavy buckets, then
+                        rng.integers(8192, 1 << 20, 3000)]),  # many light ones in the last chunks
+        rng.integers(0, top, 5000),                           # sparse: whole-key passes
+        np.array([top - 1, 0, top - 1, 5]),                  # extremes
+        np.array([], dtype=np.int64),                         # empty
+    ]
+    rows = np.array([len(x) for x in parts], dtype=np.int64)
+    off = np.zeros(len(parts) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(rows)
+    keys = np.concatenate(parts).astype(np.int32)
+    vals = rng.standard_normal(int(off[-1])).astype(np.float32)
+    b = batch_partition_groupby(keys, vals, off, num_partitions=256, key_bits=key_bits)
+    _check_batch(b, off, keys, vals, 256)
+
+
 def test_batch_graph_replay(P):
     """One CUDA-graph capture, replayed on new data in the same buffers."""
     import torch
