@@ -235,7 +235,7 @@ int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out,
                      int mode, int32_t* learned_used, void* workspace, size_t workspace_bytes,
                      void* stream);
 
-/* Many independent queries in one launch sequence (no host synchronisation,
+/* Many independent queries in one kernel launch (no host synchronisation,
  * so it can be captured in one CUDA graph).  Query q owns rows
  * [query_offsets[q], query_offsets[q+1]) of keys/values (device int64[nq+1];
  * n = query_offsets[nq], given by the host).  Per query it computes the
@@ -250,8 +250,8 @@ int jfx_learned_sort(const uint64_t* keys, int64_t n, uint64_t* sorted_keys_out,
  *   ascending.
  * Keys must lie in [0, 2^key_bits); jfx_batch_status reports a violation.
  * One persistent kernel launch does all of it: a device work queue of the
- * queries, largest first, each query's partition, sort and groupby run by
- * one CTA. */
+ * queries, largest first, each query's partition, bucket pass and groupby
+ * run by one CTA; group sums are accumulated in float64 and rounded once. */
 int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const int64_t* query_offsets,
                                 int nq, int64_t n, int num_partitions, int key_bits,
                                 int32_t* part_keys_out, float* part_values_out,
