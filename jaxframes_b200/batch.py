@@ -4,9 +4,10 @@ One call (``jfx_batch_partition_groupby``) runs, for every query, the
 one-device body of ``collective_hash_repartition`` with P partitions
 (parallel_algorithms.py:163-182, :213-214) and
 ``SortBasedGroupBy.groupby_aggregate`` sum and count (:733-803), on all
-queries' rows at once.  The launch sequence never synchronises with the host,
-so ``BatchedGroupBy.capture()`` records it as one CUDA graph and ``replay()``
-re-runs it on new data placed in the same input buffers.
+queries' rows at once, in one persistent kernel launch (a device work queue
+of the queries, one CTA per query).  The launch never synchronises with the
+host, so ``BatchedGroupBy.capture()`` records it as one CUDA graph and
+``replay()`` re-runs it on new data placed in the same input buffers.
 """
 
 from __future__ import annotations

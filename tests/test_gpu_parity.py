@@ -447,6 +447,27 @@ def _c4_like(n):
     return bench.c4_keys(nblocks=max(1, n // 4096))
 
 
+def test_every_visible_device(P):
+    """Kernels that need more than 48 KB of shared memory (the bucket sorts,
+    the batch kernel) get that attribute on each device they run on: the
+    learned sort and a small batch on every visible GPU, in turn."""
+    from jaxframes_b200.batch import batch_partition_groupby
+    rng = np.random.default_rng(77)
+    k = rng.integers(0, 2**63, 1 << 20, dtype=np.uint64)
+    ep = np.argsort(k, kind="stable")
+    rows, off, keys, vals = _batch_inputs(12, 78)
+    for d in range(torch.cuda.device_count()):
+        with torch.cuda.device(d):
+            sk, perm, used = P.learned_sort(k, mode="auto")
+            assert used == 1, f"device {d}: learned path not taken (code {used})"
+            np.testing.assert_array_equal(_np(perm), ep, err_msg=f"device {d}")
+            kt = torch.from_numpy(keys).to(f"cuda:{d}")
+            vt = torch.from_numpy(vals).to(f"cuda:{d}")
+            ot = torch.from_numpy(off).to(f"cuda:{d}")
+            b = batch_partition_groupby(kt, vt, ot, num_partitions=64)
+            _check_batch(b, off, keys, vals, 64)
+
+
 @pytest.mark.parametrize("dist", ["c4", "uniform", "sorted", "reversed", "equal", "few", "narrow"])
 def test_learned_sort_matches_plain_and_oracle(P, dist):
     """The learned-CDF sort's output is the plain radix sort's, bit for bit."""
