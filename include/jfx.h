@@ -293,12 +293,16 @@ int jfx_get_tuning(jfx_tuning* t);
  *                     check failed / large-bucket list full) as if its own
  *                     check had found it; the output is the plain sort's;
  *   fail_workspace:   1: every entry point that takes a workspace reports it
- *                     as too small (JFX_ERR_ALLOC) before launching anything. */
+ *                     as too small (JFX_ERR_ALLOC) before launching anything;
+ *   withhold_order:   1: the batch kernel never publishes its query order, so
+ *                     every CTA's bounded wait runs out, the kernel exits and
+ *                     jfx_batch_status returns JFX_ERR_TIMEOUT (give a short
+ *                     spin_limit_us). */
 typedef struct {
   int32_t withhold_tile;
   int32_t learned_fallback;
   int32_t fail_workspace;
-  int32_t reserved;
+  int32_t withhold_order;
 } jfx_fault;
 int jfx_set_fault(const jfx_fault* f);
 

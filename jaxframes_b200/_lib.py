@@ -67,7 +67,7 @@ class Tuning(ctypes.Structure):
 
 class Fault(ctypes.Structure):
     _fields_ = [("withhold_tile", ctypes.c_int32), ("learned_fallback", ctypes.c_int32),
-                ("fail_workspace", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fail_workspace", ctypes.c_int32), ("withhold_order", ctypes.c_int32)]
 
 
 class JoinPayload(ctypes.Structure):

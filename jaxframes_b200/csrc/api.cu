@@ -477,9 +477,12 @@ int jfx_set_fault(const jfx_fault* f) {
     return fail(JFX_ERR_ARG, "learned_fallback must be 0, -1 or -3, got %d", f->learned_fallback);
   if (f->fail_workspace != 0 && f->fail_workspace != 1)
     return fail(JFX_ERR_ARG, "fail_workspace must be 0 or 1, got %d", f->fail_workspace);
+  if (f->withhold_order != 0 && f->withhold_order != 1)
+    return fail(JFX_ERR_ARG, "withhold_order must be 0 or 1, got %d", f->withhold_order);
   g_fault.withhold_tile = f->withhold_tile;
   g_fault.learned_fallback = f->learned_fallback;
   g_fault.fail_workspace = f->fail_workspace;
+  g_fault.withhold_order = f->withhold_order;
   return JFX_OK;
 }
 
@@ -1591,6 +1594,7 @@ int jfx_batch_partition_groupby(const int32_t* keys, const float* values, const 
   qa.ctl = bb.ctl;
   qa.err = c.err;
   qa.spin_ns = (u64)g_tuning.spin_limit_us * 1000ull;
+  qa.withhold_order = g_fault.withhold_order ? 1u : 0u;
   k_batch_queue<<<grid, kQueueThreads, smem, s>>>(qa), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;

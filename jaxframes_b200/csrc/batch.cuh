@@ -70,6 +70,7 @@ struct QueueArgs {
   u32* ctl;              // [0] ticket, [1] queries done, [2] order ready, [3] offsets ready (zeroed)
   u32* err;
   u64 spin_ns;
+  u32 withhold_order;    // failure injection: CTA 0 never publishes the query order
 };
 
 // Bounded wait (thread 0) until *p >= target; false after spin_ns without
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(kQueueThreads, 2) k_batch_queue(QueueArgs a) {
     }
     __threadfence();
     __syncthreads();
-    if (tid == 0) atomicExch(&a.ctl[2], 1u);
+    if (tid == 0 && !a.withhold_order) atomicExch(&a.ctl[2], 1u);
   }
   if (tid == 0) S.flag[1] = queue_wait(&a.ctl[2], 1u, a.err, a.spin_ns) ? 1u : 0u;
   __syncthreads();

@@ -1668,6 +1668,7 @@ struct Fault {
   int withhold_tile = 0;
   int learned_fallback = 0;
   int fail_workspace = 0;
+  int withhold_order = 0;
 };
 extern thread_local Fault g_fault;
 

@@ -28,8 +28,9 @@ def lib():
 
 
 @contextlib.contextmanager
-def fault(lib, withhold_tile=0, learned_fallback=0, fail_workspace=0):
-    _lib.check(lib.jfx_set_fault(ctypes.byref(_lib.Fault(withhold_tile, learned_fallback, fail_workspace, 0))))
+def fault(lib, withhold_tile=0, learned_fallback=0, fail_workspace=0, withhold_order=0):
+    f = _lib.Fault(withhold_tile, learned_fallback, fail_workspace, withhold_order)
+    _lib.check(lib.jfx_set_fault(ctypes.byref(f)))
     try:
         yield
     finally:
@@ -54,6 +55,7 @@ def test_fault_and_tuning_arguments_are_checked(lib):
     assert lib.jfx_set_fault(ctypes.byref(_lib.Fault(0, -7, 0, 0))) == ARG
     assert lib.jfx_set_fault(ctypes.byref(_lib.Fault(0, -2, 0, 0))) == ARG
     assert lib.jfx_set_fault(ctypes.byref(_lib.Fault(0, 0, 2, 0))) == ARG
+    assert lib.jfx_set_fault(ctypes.byref(_lib.Fault(0, 0, 0, 2))) == ARG
     assert lib.jfx_set_fault(None) == 0
     t = _lib.Tuning()
     assert lib.jfx_get_tuning(ctypes.byref(t)) == 0
@@ -196,3 +198,40 @@ def test_short_output_capacity_is_reported(lib):
     want = np.r_[np.arange(50), np.arange(80, 100)]
     np.testing.assert_array_equal(out[:70].cpu().numpy(), want)
     del ws
+
+
+@pytest.mark.gpu
+def test_withheld_batch_order_times_out_and_the_next_batch_is_correct(lib):
+    """Every CTA of the batch kernel waits for the query order CTA 0
+    publishes; when it is withheld, their bounded waits run out, the kernel
+    exits and the status reports JFX_ERR_TIMEOUT.  The next batch on the same
+    buffers is correct."""
+    _need_gpu()
+    from jaxframes_b200.batch import BatchedGroupBy
+    from oracle import jfx_oracle as O
+    rng = np.random.default_rng(91)
+    nq = 16
+    off = np.zeros(nq + 1, dtype=np.int64)
+    off[1:] = np.cumsum(rng.integers(100, 5000, nq))
+    n = int(off[-1])
+    keys = rng.integers(0, 1000, n).astype(np.int32)
+    vals = rng.standard_normal(n).astype(np.float32)
+    b = BatchedGroupBy(n, nq, 64, 10)
+    b.keys[:n].copy_(torch.from_numpy(keys))
+    b.values[:n].copy_(torch.from_numpy(vals))
+    b.query_offsets.copy_(torch.from_numpy(off))
+    with spin_limit(lib, 2000), fault(lib, withhold_order=1):
+        b.run()
+        with pytest.raises(_lib.JfxError) as e:
+            b.status()
+    assert e.value.status == TIMEOUT
+    b.run()
+    b.status()
+    for q in range(nq):
+        k, v = keys[off[q]:off[q + 1]], vals[off[q]:off[q + 1]]
+        po, pk, pv, gk, gs, gc = (t.cpu().numpy() for t in b.query(q))
+        _, perm, eoffs = O.hash_partition([k], 64)
+        assert np.array_equal(po, eoffs) and np.array_equal(pk, k[perm]) and np.array_equal(pv, v[perm])
+        ek, eo = O.groupby_aggregate(k, {"s": v, "c": v}, {"s": "sum", "c": "count"})
+        assert np.array_equal(gk, ek) and np.array_equal(gc, eo["c"])
+        np.testing.assert_allclose(gs, eo["s"], rtol=1e-5, atol=1e-4)
