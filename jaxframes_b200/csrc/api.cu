@@ -136,7 +136,8 @@ static int launch_group_reduce(GroupArgs& ga, GroupBuffers& g, u64 n, cudaStream
   JFX_CUDA(cudaMemsetAsync(g.slot_gid, 0xff, ga.nslots * sizeof(u32), s));
   k_group_reduce<K><<<blocks, 256, 0, s>>>(ga, g.nwarps), note_launch();
   JFX_CUDA(cudaGetLastError());
-  k_group_fixup<<<(unsigned)((ga.nslots * 32 + 255) / 256), 256, 0, s>>>(ga), note_launch();
+  const u64 fix_blocks = std::min<u64>((ga.nslots + 255) / 256, (u64)device_sm_count() * 16);
+  k_group_fixup<<<(unsigned)std::max<u64>(fix_blocks, 1), 256, 0, s>>>(ga), note_launch();
   JFX_CUDA(cudaGetLastError());
   return JFX_OK;
 }

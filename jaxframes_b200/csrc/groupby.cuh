@@ -551,34 +551,46 @@ __device__ void fixup_column(const GroupArgs& a, int c, u64 i, u64 end, u32 g, i
   if (lane == 0) agg_finalize<KIND>(a.v[c], g, s);
 }
 
-// One warp per partial record; the warp of the record holding the group's
-// first row finds the group's following records (same group id, not a group
-// start; empty records in between) 32 at a time and combines them.
+// For every partial record that holds a group's first row, a warp finds the
+// group's following records (same group id, not a group start; empty
+// records in between) 32 at a time and combines them.  Warps take the
+// records 32 at a time over a grid sized to the GPU, so the mostly empty or
+// continuing records cost a ballot, not a warp launch each.
 __global__ void __launch_bounds__(256) k_group_fixup(GroupArgs a) {
-  const u64 i = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // a warp takes 32 records at a time (grid-stride) and handles the ones
+  // that hold a group's first row, one after the other
   const int lane = threadIdx.x & 31;
-  if (i >= a.nslots) return;  // whole warps
-  const u32 g = a.slot_gid[i];
-  if (g == kEmptySlot || !a.slot_started[i]) return;
-  u64 end = a.nslots;
-  for (u64 b = i + 1; b < a.nslots; b += 32) {
-    const u64 j = b + lane;
-    bool stop = j >= a.nslots;
-    if (!stop) {
-      const u32 gj = a.slot_gid[j];
-      stop = gj != kEmptySlot && (gj != g || a.slot_started[j]);
-    }
-    const u32 sm = __ballot_sync(0xffffffffu, stop);
-    if (sm) {
-      end = b + __ffs(sm) - 1;
-      break;
-    }
-  }
-  for (int c = 0; c < a.nvals; ++c) {
-    switch (a.v[c].kind) {
-      case VK_F: fixup_column<VK_F>(a, c, i, end, g, lane); break;
-      case VK_I: fixup_column<VK_I>(a, c, i, end, g, lane); break;
-      default: fixup_column<VK_U>(a, c, i, end, g, lane); break;
+  const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 base = (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < a.nslots; base += nw * 32) {
+    const u64 jl = base + lane;
+    const u32 gl = jl < a.nslots ? a.slot_gid[jl] : kEmptySlot;
+    u32 todo = __ballot_sync(0xffffffffu, gl != kEmptySlot && a.slot_started[jl]);
+    while (todo) {
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const u64 i = base + l;
+      const u32 g = __shfl_sync(0xffffffffu, gl, l);
+      u64 end = a.nslots;
+      for (u64 b = i + 1; b < a.nslots; b += 32) {
+        const u64 j = b + lane;
+        bool stop = j >= a.nslots;
+        if (!stop) {
+          const u32 gj = a.slot_gid[j];
+          stop = gj != kEmptySlot && (gj != g || a.slot_started[j]);
+        }
+        const u32 sm = __ballot_sync(0xffffffffu, stop);
+        if (sm) {
+          end = b + __ffs(sm) - 1;
+          break;
+        }
+      }
+      for (int c = 0; c < a.nvals; ++c) {
+        switch (a.v[c].kind) {
+          case VK_F: fixup_column<VK_F>(a, c, i, end, g, lane); break;
+          case VK_I: fixup_column<VK_I>(a, c, i, end, g, lane); break;
+          default: fixup_column<VK_U>(a, c, i, end, g, lane); break;
+        }
+      }
     }
   }
 }
