@@ -574,6 +574,21 @@ def test_batch_key_spreads(P, key_bits):
     _check_batch(b, off, keys, vals, 256)
 
 
+def test_batch_more_queries_than_the_device_orders(P):
+    """Over 4096 queries the work queue takes them in index order instead of
+    largest first; results are the same."""
+    from jaxframes_b200.batch import batch_partition_groupby
+    rng = np.random.default_rng(93)
+    rows = rng.integers(0, 60, 5000)
+    rows[::11] = 0
+    off = np.zeros(len(rows) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(rows)
+    keys = rng.integers(0, 40, int(off[-1])).astype(np.int32)
+    vals = rng.standard_normal(int(off[-1])).astype(np.float32)
+    b = batch_partition_groupby(keys, vals, off, num_partitions=16)
+    _check_batch(b, off, keys, vals, 16)
+
+
 def test_batch_graph_replay(P):
     """One CUDA-graph capture, replayed on new data in the same buffers."""
     import torch
