@@ -3,8 +3,9 @@
  * algorithms layer (src/jaxframes/distributed/parallel_algorithms.py).
  *
  * Every entry point takes plain device pointers, element counts, a caller-owned
- * device workspace (size from jfx_workspace_size) and a cudaStream_t passed as
- * void*.  Work is stream-ordered; entry points that must size an output (group
+ * device workspace (size from jfx_workspace_size, 256-byte aligned as
+ * cudaMalloc returns it; a misaligned one is JFX_ERR_ARG) and a cudaStream_t
+ * passed as void*.  Work is stream-ordered; entry points that must size an output (group
  * count, join pair count) synchronise the stream once and return the size
  * through a host pointer, as the reference does with its host reads at
  * parallel_algorithms.py:712, :772 and :880.

@@ -194,6 +194,8 @@ struct Leaf {
   u32 lo, hi;    // the leaf's position range [lo, hi)
 };
 
+static_assert(sizeof(Leaf) == 32, "model_pos loads a leaf as two 16-byte words");
+
 struct ModelRef {
   double ra, rb;       // leaf coordinate = ra * feature(x) + rb
   const Leaf* leaves;  // [kLeaves]
@@ -213,10 +215,13 @@ __device__ __forceinline__ int model_leaf(const ModelRef& m, u64 x) {
 
 // Predicted output position of key x: monotone non-decreasing in x.
 __device__ __forceinline__ u32 model_pos(const ModelRef& m, u64 x) {
-  const Leaf* lp = m.leaves + model_leaf(m, x);
-  const u64 x0 = __ldg(&lp->x0);
-  const double slope = __ldg(&lp->slope), base = __ldg(&lp->base);
-  const u32 lo = __ldg(&lp->lo), hi = __ldg(&lp->hi);
+  // the 32-byte leaf in two 16-byte loads (the leaf table is 256-byte aligned)
+  const uint4* lp = reinterpret_cast<const uint4*>(m.leaves + model_leaf(m, x));
+  const uint4 w0 = __ldg(lp), w1 = __ldg(lp + 1);
+  const u64 x0 = (u64)w0.x | ((u64)w0.y << 32);
+  const double slope = __longlong_as_double((long long)((u64)w0.z | ((u64)w0.w << 32)));
+  const double base = __longlong_as_double((long long)((u64)w1.x | ((u64)w1.y << 32)));
+  const u32 lo = w1.z, hi = w1.w;
   const double d = x >= x0 ? (double)(x - x0) : -(double)(x0 - x);
   const double p = base + slope * d;
   const u32 top = hi > lo ? hi - 1 : lo;
@@ -1677,6 +1682,10 @@ inline int check_workspace(const Arena& ar, const void* workspace, size_t bytes)
   if (ar.overflow || !workspace || g_fault.fail_workspace)
     return fail(JFX_ERR_ALLOC, "workspace of %zu bytes < %zu needed%s", bytes, ar.off,
                 g_fault.fail_workspace ? " (failure injected by jfx_set_fault)" : "");
+  // the carve hands out 256-byte offsets and kernels load 16-byte vectors
+  // from them, so the base must be aligned as cudaMalloc returns it
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+    return fail(JFX_ERR_ARG, "workspace %p is not 256-byte aligned", workspace);
   return JFX_OK;
 }
 

@@ -83,6 +83,20 @@ def test_injected_workspace_failure_stops_before_any_launch(lib):
     assert lib.jfx_launch_count() == launches
 
 
+def test_misaligned_workspace_is_rejected_before_any_launch(lib):
+    """The workspace carve hands out 256-byte offsets and kernels load 16-byte
+    vectors from them: a base that is not 256-byte aligned is an argument
+    error, found on the host before the device is touched."""
+    fake = ctypes.c_void_p(1 << 40)
+    bad = ctypes.c_void_p((1 << 40) + 16)
+    col = _lib.Column(fake, _lib.I64, 0)
+    launches = lib.jfx_launch_count()
+    assert lib.jfx_sort(ctypes.byref(col), 1000, 1, fake, None, bad, 1 << 30, None) == ARG
+    assert b"aligned" in lib.jfx_last_error()
+    assert lib.jfx_learned_sort(fake, 1000, fake, fake, 0, None, bad, 1 << 30, None) == ARG
+    assert lib.jfx_launch_count() == launches
+
+
 # ------------------------------------------------------------------ GPU ---
 def _need_gpu():
     if not torch.cuda.is_available():
