@@ -1435,7 +1435,7 @@ int jfx_learned_sort(const uint64_t* keys_in, int64_t n, uint64_t* sorted_out_in
   // 4. sort inside every bucket: most by k_bucket_sort<8>, those of 2049 to
   // 4096 rows by k_bucket_sort<16>, which lists the larger ones
   JFX_CUDA(cudaMemsetAsync(l.bcounts, 0, 8 * sizeof(u32), s));
-  k_bucket_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(l.spos, N, (u32)l.nb, l.starts), note_launch();
+  k_bucket_starts<<<grid_for(N / 4 + 1, 256), 256, 0, s>>>(l.spos, N, (u32)l.nb, l.starts), note_launch();
   {
     static SmemAttr attr8, attr16;
     JFX_TRY(ensure_smem(attr8, k_bucket_sort<8>, bucket_smem<8>()));

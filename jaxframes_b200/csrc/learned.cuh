@@ -203,11 +203,34 @@ constexpr u32 kLargeChunk = 1u << 16;   // rows per CTA of the large buckets' mi
 
 // starts[c] = first row of bucket c in the bucket-sorted ids sb[0..n), for
 // c in [0, nb]; an empty bucket starts where the next non-empty one does.
+// Thread t takes rows 4t .. 4t + 3 with one 16-byte load (sb is 256-byte
+// aligned), and the thread whose rows reach n also writes the buckets that
+// start at n (the empty ones after the last row).
 __global__ void k_bucket_starts(const u32* sb, u64 n, u32 nb, u32* starts) {
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (u64)gridDim.x * blockDim.x) {
-    const u32 lo = i == 0 ? 0u : sb[i - 1] + 1u;  // buckets that start at row i
-    const u32 hi = i == n ? nb : sb[i];
-    for (u32 c = lo; c <= hi && c <= nb; ++c) starts[c] = (u32)i;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; 4 * t <= n; t += stride) {
+    const u64 i0 = 4 * t;
+    u32 v[4];
+    if (i0 + 4 <= n) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(sb) + t);
+      v[0] = q.x;
+      v[1] = q.y;
+      v[2] = q.z;
+      v[3] = q.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = i0 + k < n ? sb[i0 + k] : nb;
+    }
+    u32 prev = i0 == 0 ? 0xffffffffu : __ldg(sb + i0 - 1);  // lo = prev + 1 wraps to 0 for row 0
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const u64 i = i0 + k;
+      if (i > n) break;
+      const u32 lo = prev + 1u;  // buckets that start at row i
+      const u32 hi = i == n ? nb : v[k];
+      for (u32 c = lo; c <= hi && c <= nb; ++c) starts[c] = (u32)i;
+      prev = v[k];
+    }
   }
 }
 
@@ -227,7 +250,20 @@ __device__ __forceinline__ void block_minmax(const u64* keys, u32 s, u32 e, u64*
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   mn = ~0ull;
   mx = 0ull;
-  for (u32 j = s + threadIdx.x; j < e; j += blockDim.x) {
+  // eight independent loads in flight per thread, then the remainder
+  constexpr int U = 8;
+  u32 j = s + threadIdx.x;
+  for (; j + (U - 1) * blockDim.x < e; j += U * blockDim.x) {
+    u64 k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) k[u] = __ldg(keys + j + u * blockDim.x);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      mn = k[u] < mn ? k[u] : mn;
+      mx = k[u] > mx ? k[u] : mx;
+    }
+  }
+  for (; j < e; j += blockDim.x) {
     const u64 k = keys[j];
     mn = k < mn ? k : mn;
     mx = k > mx ? k : mx;
