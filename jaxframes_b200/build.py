@@ -24,7 +24,10 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr",
     "-Xcudafe", "--diag_suppress=177",
-    "-split-compile=0",  # optimise the kernels in parallel, one job per host core
+    # optimise the kernels in parallel in a fixed number of jobs: how the
+    # module is split between the jobs shapes the generated code, so the
+    # count does not follow the building machine's cores
+    "-split-compile=8",
 ]
 
 
