@@ -536,7 +536,7 @@ def _check_batch(b, off, keys, vals, P):
             assert (np.abs(_np(gs).astype(np.float64) - eo["s"]) <= asum * 2.0 ** -16 + 1e-30).all(), q
 
 
-@pytest.mark.parametrize("P_", [256, 7])
+@pytest.mark.parametrize("P_", [256, 7, 1])
 def test_batch_partition_groupby(P, P_):
     from jaxframes_b200.batch import batch_partition_groupby
     rows, off, keys, vals = _batch_inputs(40, 5 + P_)
