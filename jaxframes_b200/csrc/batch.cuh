@@ -99,6 +99,12 @@ __device__ __forceinline__ bool queue_wait(const u32* p, u32 target, u32* err, u
   }
 }
 
+// Partition of a key: fmix32(key) % P, a mask when P is a power of two.
+__device__ __forceinline__ u32 part_of(u32 key, u32 P) {
+  const u32 h = fmix32_d(key);
+  return (P & (P - 1u)) == 0u ? (h & (P - 1u)) : h % P;
+}
+
 struct QueueShared {
   u32 whist[8 * 256];
   u32 wmask[8 * 256];
@@ -148,7 +154,7 @@ __device__ void queue_hist(QueueShared& S, const u32* ks, u64 q0, u64 q1, u32 P,
       bad |= valid && k[i] > lim;
       mx = valid && k[i] > mx ? k[i] : mx;
       for (int b = 0; b <= ndig; ++b) {
-        const u32 d = b == 0 ? fmix32_d(k[i]) % P : (k[i] >> (kWinBits + 8 * (b - 1))) & 255u;
+        const u32 d = b == 0 ? part_of(k[i], P) : (k[i] >> (kWinBits + 8 * (b - 1))) & 255u;
         const u32 d0 = __shfl_sync(0xffffffffu, d, 0);
         if (__all_sync(0xffffffffu, !valid || d == d0)) {
           if (lane == 0) atomicAdd(&S.hist[256 * b + d0], (u32)__popc(vb));
@@ -530,7 +536,7 @@ __global__ void __launch_bounds__(kQueueThreads, 2) k_batch_queue(QueueArgs a) {
     const bool dense = kbits <= kWinBits || q1 - q0 >= (kDenseRowsPerBucket << (kbits - kWinBits));
     u32* part_k = (u32*)a.part_keys;
     u32* part_v = (u32*)a.part_values;
-    const auto pdig = [P](u32 kk) { return fmix32_d(kk) % P; };
+    const auto pdig = [P](u32 kk) { return part_of(kk, P); };
     const u32* ks = part_k;
     const u32* vs = part_v;
     int pp = 0;
