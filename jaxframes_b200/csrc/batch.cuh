@@ -121,7 +121,7 @@ struct QueueShared {
   u32 q;
   // groups: float64 sums and counts of a chunk (sorted rows) or of a window
   // of kWin keys (bucketed rows); passes: the chunk's keys and values staged
-  // in digit order (lsum) and their digits (lcnt)
+  // in digit order (lsum)
   double lsum[kQueueChunk + 1];
   u32 lcnt[kQueueChunk + 1];
 };
@@ -226,7 +226,6 @@ __device__ __forceinline__ void chunk_scatter(QueueShared& S, u32* base, const u
   block_exclusive_scan<kQueueThreads, RADIX>(S.cexcl, S.scan);  // the chunk's digit starts
   u32* stk = reinterpret_cast<u32*>(S.lsum);
   u32* stv = stk + kQueueChunk;
-  unsigned char* sdg = reinterpret_cast<unsigned char*>(S.lcnt);
 #pragma unroll
   for (int i = 0; i < IPT; ++i) {
     if (rd[i] != kNoRank) {
@@ -234,19 +233,19 @@ __device__ __forceinline__ void chunk_scatter(QueueShared& S, u32* base, const u
       const u32 pos = S.cexcl[d] + wh[d] + (rd[i] & 0xffffu);
       stk[pos] = k[i];
       stv[pos] = v[i];
-      sdg[pos] = (unsigned char)d;
     }
   }
   __syncthreads();
   const u32 cn = (u32)min((u64)kQueueChunk, q1 - c0);
   for (u32 j = tid; j < cn; j += kQueueThreads) {
-    const u32 d = sdg[j];
+    const u32 kk = stk[j];
+    const u32 d = dig(kk);  // recomputed from the staged key (cheaper than staging it)
     const u64 dst = q0 + base[d] + (j - S.cexcl[d]);
     if (dst >= q1) {  // only reachable if the counts and the pass disagree
       atomicOr(err, DERR_BOUNDS);
       continue;
     }
-    dk[dst] = stk[j];
+    dk[dst] = kk;
     dv[dst] = stv[j];
   }
   __syncthreads();
