@@ -249,8 +249,9 @@ __device__ __forceinline__ void chunk_scatter(QueueShared& S, u32* base, const u
     dv[dst] = stv[j];
   }
   __syncthreads();
+  // thread d advances digit d's base; the next chunk reads it only after its
+  // ranking barrier, and a reader after the pass synchronises first
   base[tid] += S.tot[tid];
-  __syncthreads();
 }
 
 // A stable pass of rows [q0, q1) of (ks, vs) by dig1 into (dk1, dv1) whose
@@ -572,6 +573,7 @@ __global__ void __launch_bounds__(kQueueThreads, 2) k_batch_queue(QueueArgs a) {
     }
     // hist row 0 now holds each partition's end; a partition starts where
     // the previous one ends
+    __syncthreads();
     if (tid < (int)P) a.part_offsets[(u64)q * (P + 1) + tid] = (int64_t)(q0 + (tid ? S.hist[tid - 1] : 0u));
     if (tid == 0) a.part_offsets[(u64)q * (P + 1) + P] = (int64_t)q1;
     // 1c. groups: a shared-memory table per bucket, or boundaries of the
